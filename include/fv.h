@@ -1,0 +1,147 @@
+/*
+ * fv.h -- C-ABI of the B200 (sm_100a) finite-volume solver for the 2D compressible Euler equations.
+ *
+ * This is the drop-in boundary for the solver step of GusGus2004/neural-pde-surrogate.  The
+ * reference's in-process interface is the C++ class e2d::Solver
+ *     Solver(const Grid&, FluxFn, Limiter, double cfl)       solver/src/solver2d.hpp:61-64
+ *     double compute_dt(const std::vector<Conserved>& U)     solver/src/solver2d.hpp:67-83
+ *     void   step(std::vector<Conserved>& U, double dt)      solver/src/solver2d.hpp:86-103
+ * with the plug-in points FluxFn (riemann2d.hpp:8) and Limiter (limiters.hpp:5) chosen by name in
+ * the driver (main2d.cpp:145-155), the grid of make_grid (grid2d.hpp:30-39), the driver's frame
+ * loop (main2d.cpp:224-246) and TrajectoryWriter::add (trajectory.hpp:31-51).  Each entry point
+ * below names the piece it replaces.
+ *
+ * Conventions
+ *  - Plain C types only.  Every function returns an int status (FV_OK or an FV_ERR_* code) and never
+ *    exits the process; fv_last_error() gives a message for the calling thread's last failure.
+ *  - State layout: interior cells only, row-major, 4 doubles per cell (rho, rho*u, rho*v, E), i.e.
+ *    U[(j*nx + i)*4 + q] -- the reference's std::vector<Conserved> without the 2-cell ghost ring.
+ *    Ghost cells are never stored: boundaries are applied inside the kernels.
+ *  - Host buffers are owned by the caller; device buffers by the library.  Functions whose name
+ *    ends in _device take device pointers (no host copies).
+ *  - One handle must not be used from two threads at once (the reference Solver is not reentrant
+ *    either: shared scratch, solver2d.hpp:110-113).  All work runs on the handle's stream.
+ *  - Results are bit-identical to the reference's CPU solver for every tile shape and grid size.
+ */
+#ifndef FV_H
+#define FV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FV_OK 0
+#define FV_ERR_ARG 1         /* invalid argument (the driver's "must be positive" / unknown-name errors) */
+#define FV_ERR_CUDA 2        /* CUDA runtime error, or no usable GPU */
+#define FV_ERR_NONPHYSICAL 3 /* !(rho > 0) || !(p > 0) in a cell (solver2d.hpp:75); the reference exits(1) */
+#define FV_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define FV_ERR_STATE 5       /* call out of order (e.g. no state set) */
+
+/* boundary conditions (grid2d.hpp:7) */
+#define FV_BC_TRANSMISSIVE 0
+#define FV_BC_PERIODIC 1
+/* flux schemes (main2d.cpp:145-148) */
+#define FV_FLUX_RUSANOV 0
+#define FV_FLUX_HLLC 1
+/* limiters (main2d.cpp:150-155) */
+#define FV_LIM_NONE 0
+#define FV_LIM_UNLIMITED 1
+#define FV_LIM_MINMOD 2
+#define FV_LIM_VANLEER 3
+
+typedef struct fv_solver fv_solver;
+
+/* First non-physical cell in row-major order (report_bad_cell, solver2d.hpp:116-126). */
+typedef struct {
+    int i, j;
+    double rho, p;
+} fv_bad_cell;
+
+/* Replaces make_grid (grid2d.hpp:30-39) + Solver::Solver (solver2d.hpp:61-64).  Allocates the state
+ * and scratch on the current CUDA device once.  stream: a cudaStream_t, or NULL for a stream the
+ * library creates. */
+int fv_create(int nx, int ny, double x_min, double x_max, double y_min, double y_max, int bc_x, int bc_y,
+              int flux, int limiter, double cfl, void* stream, fv_solver** out);
+int fv_destroy(fv_solver* s);
+
+/* Conserved state in/out (interior cells, layout above).  Setting the state resets t and the step
+ * count to 0 unless fv_set_time is called after it. */
+int fv_set_state(fv_solver* s, const double* U);
+int fv_get_state(fv_solver* s, double* U);
+int fv_set_state_device(fv_solver* s, const double* dU);
+int fv_get_state_device(fv_solver* s, double* dU);
+/* Primitive (rho, u, v, p), each an (ny, nx) array, converted with to_conserved (state2d.hpp:16-19)
+ * as read_initial_condition does (io_hdf5.hpp:197-204).  Returns FV_ERR_ARG if any rho or p is not
+ * positive (io_hdf5.hpp:201-202) and leaves the state unchanged. */
+int fv_set_primitive(fv_solver* s, const double* rho, const double* u, const double* v, const double* p);
+
+/* Simulation time and step count kept on the device by fv_advance_to. */
+int fv_set_time(fv_solver* s, double t);
+int fv_get_time(fv_solver* s, double* t, long long* steps);
+
+/* Replaces Solver::compute_dt (solver2d.hpp:67-83): dt = cfl / (sx/dx + sy/dy).  On a non-physical
+ * cell returns FV_ERR_NONPHYSICAL and fills *bad (may be NULL) instead of exiting. */
+int fv_compute_dt(fv_solver* s, double* dt, fv_bad_cell* bad);
+
+/* Replaces Solver::step (solver2d.hpp:86-103): one SSP-RK2 step with the given dt.  Like the
+ * reference's step it does not advance the simulation time (the driver does); it does count the step. */
+int fv_step(fv_solver* s, double dt);
+
+/* The driver's inner loop (main2d.cpp:237-242): while (t < t_next) { dt = min(compute_dt(U),
+ * t_next - t); step(U, dt); t += dt; } -- run on the device, with dt never leaving the GPU.  Returns
+ * FV_ERR_NONPHYSICAL (and *bad) where compute_dt would have exited; the state is then the one that
+ * failed the check.  t and steps (may be NULL) receive the new time and total step count. */
+int fv_advance_to(fv_solver* s, double t_next, double* t, long long* steps, fv_bad_cell* bad);
+
+/* Replaces TrajectoryWriter::add for one storage level (trajectory.hpp:31-51): f x f block sums in
+ * FP64 (j-outer, i-inner) times 1/(f*f), cast to float, layout (4, ny/f, nx/f).  f must divide nx
+ * and ny (trajectory.hpp:19-28), else FV_ERR_ARG. */
+int fv_block_average(fv_solver* s, int factor, float* out);
+int fv_block_average_device(fv_solver* s, int factor, float* d_out);
+
+/* Whole trajectory in one call (main2d.cpp:224-246 in --traj mode): spin up silently to t_start,
+ * record frame 0, then nout frames at t_start + (t_end - t_start)*k/nout, each block-averaged to
+ * every size in sizes[0..nsizes-1] (a size m means factor nx/m, trajectory.hpp:19-28).  out[l]
+ * receives (nout+1, 4, ny/f, nx/f) floats for level l; times (may be NULL) receives nout+1 doubles.
+ * *steps (may be NULL) receives the total step count. */
+int fv_run_trajectory(fv_solver* s, double t_start, double t_end, int nout, const int* sizes, int nsizes,
+                      float** out, double* times, long long* steps, fv_bad_cell* bad);
+
+/* Face fluxes of n face pairs evaluated on the GPU by the same device code the stage kernels use:
+ * the FluxFn (riemann2d.hpp:8; rusanov_flux :11-15, hllc_flux :27-39) for y_face = 0, or
+ * flux_y_face (riemann2d.hpp:42-44) for y_face = 1.  UL, UR, F: host arrays of n x 4 doubles.
+ * Inspection hook for the Riemann solvers (the reference's test_riemann2d.cpp calls them directly). */
+int fv_riemann_flux(int flux, int y_face, int n, const double* UL, const double* UR, double* F);
+
+/* The (ny+4) x (nx+4) ghosted array that apply_bcs (grid2d.hpp:43-66) builds from the interior
+ * state U, produced on the GPU with the boundary mapping the stage kernels use (no ghost ring is
+ * stored by the solver itself).  Ug: host array of (ny+4)*(nx+4)*4 doubles. */
+int fv_fill_ghosts(int nx, int ny, int bc_x, int bc_y, const double* U, double* Ug);
+
+/* Kernel timing (the reference's --profile, solver2d.hpp:29-52, main2d.cpp:261): while enabled,
+ * CUDA events bracket every stage-kernel launch of the handle; fv_profile_read returns the mean
+ * duration in ms of stage-1 and stage-2 launches and the number of steps timed since enabling. */
+int fv_profile(fv_solver* s, int enable);
+int fv_profile_read(fv_solver* s, double* ms_stage1, double* ms_stage2, long long* steps_timed);
+
+/* Number of kernels the handle has launched since it was created. */
+int fv_launch_count(fv_solver* s, long long* launches);
+
+/* Blocks until all work queued on the handle's stream is done. */
+int fv_synchronize(fv_solver* s);
+
+/* Message for the calling thread's last failing call ("" if none). */
+const char* fv_last_error(void);
+
+/* Library version string. */
+const char* fv_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FV_H */

@@ -1,0 +1,88 @@
+"""ctypes loader for libfv.so (include/fv.h).  No CPU fallback: if the library or a GPU is missing,
+calls raise instead of computing anything elsewhere."""
+import ctypes as C
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+
+FV_OK, FV_ERR_ARG, FV_ERR_CUDA, FV_ERR_NONPHYSICAL, FV_ERR_TIMEOUT, FV_ERR_STATE = range(6)
+
+
+class FVError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class NonPhysicalError(FVError):
+    """The state failed compute_dt's check !(rho > 0) || !(p > 0) (solver2d.hpp:75); where the
+    reference prints 'Non-physical state in cell (i, j): rho = ..., p = ...' and exits(1)."""
+
+    def __init__(self, i, j, rho, p):
+        super().__init__(FV_ERR_NONPHYSICAL, f"Non-physical state in cell ({i}, {j}): rho = {rho:g}, p = {p:g}")
+        self.i, self.j, self.rho, self.p = i, j, rho, p
+
+
+class BadCell(C.Structure):
+    _fields_ = [("i", C.c_int), ("j", C.c_int), ("rho", C.c_double), ("p", C.c_double)]
+
+
+_D, _I, _P = C.c_double, C.c_int, C.c_void_p
+_DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
+_LLP = C.POINTER(C.c_longlong)
+_BP = C.POINTER(BadCell)
+
+_PROTOS = {
+    "fv_create": [_I, _I, _D, _D, _D, _D, _I, _I, _I, _I, _D, _P, C.POINTER(_P)],
+    "fv_destroy": [_P],
+    "fv_set_state": [_P, _P],
+    "fv_get_state": [_P, _P],
+    "fv_set_state_device": [_P, _P],
+    "fv_get_state_device": [_P, _P],
+    "fv_set_primitive": [_P, _P, _P, _P, _P],
+    "fv_set_time": [_P, _D],
+    "fv_get_time": [_P, _DP, _LLP],
+    "fv_compute_dt": [_P, _DP, _BP],
+    "fv_step": [_P, _D],
+    "fv_advance_to": [_P, _D, _DP, _LLP, _BP],
+    "fv_block_average": [_P, _I, _P],
+    "fv_block_average_device": [_P, _I, _P],
+    "fv_run_trajectory": [_P, _D, _D, _I, _P, _I, _P, _P, _LLP, _BP],
+    "fv_synchronize": [_P],
+    "fv_riemann_flux": [_I, _I, _I, _P, _P, _P],
+    "fv_fill_ghosts": [_I, _I, _I, _I, _P, _P],
+    "fv_profile": [_P, _I],
+    "fv_profile_read": [_P, _DP, _DP, _LLP],
+    "fv_launch_count": [_P, _LLP],
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded libfv.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        path = PKG / "libfv.so"
+        if not path.exists():
+            raise ImportError(f"{path} is missing: build it with `python {PKG / 'build.py'}` (nvcc, sm_100a)")
+        L = C.CDLL(str(path))
+        for name, args in _PROTOS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.fv_last_error.restype = C.c_char_p
+        L.fv_last_error.argtypes = []
+        L.fv_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc, bad=None):
+    """Raise the Python error for a non-zero status of a libfv call."""
+    if rc == FV_OK:
+        return
+    if rc == FV_ERR_NONPHYSICAL and bad is not None:
+        raise NonPhysicalError(bad.i, bad.j, bad.rho, bad.p)
+    raise FVError(rc, lib().fv_last_error().decode() or f"libfv error {rc}")

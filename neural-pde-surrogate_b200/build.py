@@ -1,0 +1,56 @@
+"""Build recipe for the native libraries of this package (in-tree, so the .so files travel with the
+repository snapshot).  Cross-compiles for sm_100a with nvcc; no GPU needed to build.
+
+  python neural-pde-surrogate_b200/build.py [--force] [-v]
+
+libfv.so -- the finite-volume solver (csrc/fv_api.cu + csrc/fv_kernels.cuh), C-ABI in include/fv.h.
+            Built with --fmad=false: no FMA contraction, which keeps every result bit-identical to
+            the reference CPU solver (its build uses none either).
+"""
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+NVCC = "/usr/local/cuda/bin/nvcc"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{ROOT / 'include'}"]
+
+LIBS = {
+    "libfv.so": {
+        "sources": ["fv_api.cu"],
+        "deps": ["fv_api.cu", "fv_kernels.cuh", "fv_physics.cuh"],
+        "flags": ["--fmad=false"],
+        "headers": ["fv.h"],
+    },
+}
+
+
+def _stale(out, deps, headers):
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    files = [CSRC / d for d in deps] + [ROOT / "include" / h for h in headers] + [Path(__file__)]
+    return any(f.stat().st_mtime > t for f in files)
+
+
+def build(force=False, verbose=False):
+    built = []
+    for name, spec in LIBS.items():
+        out = PKG / name
+        if not force and not _stale(out, spec["deps"], spec["headers"]):
+            continue
+        cmd = [NVCC, *ARCH, *COMMON, *spec["flags"], "-shared", "-o", str(out),
+               *[str(CSRC / s) for s in spec["sources"]], *spec.get("libs", [])]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        built.append(name)
+    return built
+
+
+if __name__ == "__main__":
+    print("built:", build(force="--force" in sys.argv, verbose="-v" in sys.argv))

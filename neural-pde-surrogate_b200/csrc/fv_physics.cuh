@@ -1,0 +1,152 @@
+// Device-side physics of the 2D Euler finite-volume step: equation of state, slope limiters, MUSCL
+// edge states and the Rusanov / HLLC face fluxes.
+//
+// Every expression keeps the operation order and association of the reference solver core
+// (GusGus2004/neural-pde-surrogate, solver/src/{state2d,limiters,riemann2d,solver2d}.hpp) so that,
+// compiled with --fmad=false, results are bit-identical to the reference's CPU build (which uses no
+// FMA contraction).  IEEE division and square root (CUDA's default `/` and `sqrt` for double) are
+// used; replacing a division with a reciprocal multiply would change the bits.
+#pragma once
+#include <cstdint>
+
+namespace fv {
+
+constexpr double GAMMA = 1.4;          // state2d.hpp:7
+constexpr double GM1 = GAMMA - 1.0;    // the double constant 0.39999999999999991 used by the reference
+
+enum : int { BC_TRANSMISSIVE = 0, BC_PERIODIC = 1 };
+enum : int { FLUX_RUSANOV = 0, FLUX_HLLC = 1 };
+enum : int { LIM_NONE = 0, LIM_UNLIMITED = 1, LIM_MINMOD = 2, LIM_VANLEER = 3 };
+
+// One cell: conserved (rho, rho*u, rho*v, E) or primitive (rho, u, v, p).  32 bytes, the same layout
+// as the reference's e2d::Conserved / e2d::Primitive (state2d.hpp:9-10).
+struct __align__(16) Q4 {
+    double a, b, c, d;
+};
+
+__device__ __forceinline__ Q4 ld_q4(const Q4* p) {
+    const double2* v = reinterpret_cast<const double2*>(p);
+    double2 x = v[0], y = v[1];
+    return Q4{x.x, x.y, y.x, y.y};
+}
+__device__ __forceinline__ void st_q4(Q4* p, const Q4& q) {
+    double2* v = reinterpret_cast<double2*>(p);
+    v[0] = make_double2(q.a, q.b);
+    v[1] = make_double2(q.c, q.d);
+}
+__device__ __forceinline__ Q4 ldg_q4(const Q4* p) {
+    const double2* v = reinterpret_cast<const double2*>(p);
+    double2 x = __ldg(v), y = __ldg(v + 1);
+    return Q4{x.x, x.y, y.x, y.y};
+}
+
+// std::min / std::max as the reference uses them (<algorithm>): min(a,b) = (b<a)?b:a, max(a,b) = (a<b)?b:a.
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+// state2d.hpp:16-19
+__device__ __forceinline__ Q4 to_conserved(const Q4& W) {
+    return Q4{W.a, W.a * W.b, W.a * W.c, W.d / GM1 + 0.5 * W.a * (W.b * W.b + W.c * W.c)};
+}
+
+// state2d.hpp:21-25
+__device__ __forceinline__ Q4 to_primitive(const Q4& U) {
+    double u = U.b / U.a, v = U.c / U.a;
+    double p = GM1 * (U.d - 0.5 * U.a * (u * u + v * v));
+    return Q4{U.a, u, v, p};
+}
+
+// state2d.hpp:27
+__device__ __forceinline__ double sound_speed(const Q4& W) { return sqrt(GAMMA * W.d / W.a); }
+
+// state2d.hpp:30-36, with the primitive state of U supplied by the caller (it is the same
+// to_primitive(U) the reference recomputes, so reusing it is bit-identical).
+__device__ __forceinline__ Q4 flux_x(const Q4& U, const Q4& W) {
+    return Q4{U.b, U.b * W.b + W.d, U.c * W.b, W.b * (U.d + W.d)};
+}
+
+// limiters.hpp:7-18
+template <int LIM>
+__device__ __forceinline__ double limiter(double a, double b) {
+    if constexpr (LIM == LIM_NONE) {
+        return 0.0;
+    } else if constexpr (LIM == LIM_UNLIMITED) {
+        return 0.5 * (a + b);
+    } else if constexpr (LIM == LIM_MINMOD) {
+        if (a * b <= 0.0) return 0.0;
+        return (fabs(a) < fabs(b)) ? a : b;
+    } else {
+        if (a * b <= 0.0) return 0.0;
+        return 2.0 * a * b / (a + b);
+    }
+}
+
+// solver2d.hpp:17-22
+template <int LIM>
+__device__ __forceinline__ Q4 limited_slope(const Q4& Wm, const Q4& W0, const Q4& Wp) {
+    return Q4{limiter<LIM>(W0.a - Wm.a, Wp.a - W0.a), limiter<LIM>(W0.b - Wm.b, Wp.b - W0.b),
+              limiter<LIM>(W0.c - Wm.c, Wp.c - W0.c), limiter<LIM>(W0.d - Wm.d, Wp.d - W0.d)};
+}
+
+// solver2d.hpp:25-27 with s = +1 (right/top edge) or -1 (left/bottom edge): W + (0.5*s)*dW.
+__device__ __forceinline__ Q4 edge(const Q4& W, const Q4& dW, double s) {
+    double h = 0.5 * s;
+    return Q4{W.a + h * dW.a, W.b + h * dW.b, W.c + h * dW.c, W.d + h * dW.d};
+}
+
+// riemann2d.hpp:11-15
+__device__ __forceinline__ Q4 rusanov_flux(const Q4& UL, const Q4& UR) {
+    Q4 WL = to_primitive(UL), WR = to_primitive(UR);
+    double s_max = smax(fabs(WL.b) + sound_speed(WL), fabs(WR.b) + sound_speed(WR));
+    Q4 FL = flux_x(UL, WL), FR = flux_x(UR, WR);
+    double h = 0.5 * s_max;
+    return Q4{0.5 * (FL.a + FR.a) - h * (UR.a - UL.a), 0.5 * (FL.b + FR.b) - h * (UR.b - UL.b),
+              0.5 * (FL.c + FR.c) - h * (UR.c - UL.c), 0.5 * (FL.d + FR.d) - h * (UR.d - UL.d)};
+}
+
+// riemann2d.hpp:27-39 (Davis wave speeds, Toro eq. 10.39 star state riemann2d.hpp:18-24).
+// The reference evaluates only the branch it returns; here the upwind side is selected first
+// (left when 0 <= SL or 0 <= S_star, as its first two branches are) and the star state is evaluated
+// once for that side, so that all lanes of a warp run one code path.  Every branch returns the same
+// expression on the same inputs as the reference, hence bit-identical results.
+__device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& UR) {
+    Q4 WL = to_primitive(UL), WR = to_primitive(UR);
+    double aL = sound_speed(WL), aR = sound_speed(WR);
+    double SL = smin(WL.b - aL, WR.b - aR);
+    double SR = smax(WL.b + aL, WR.b + aR);
+    double S_star = (WR.d - WL.d + WL.a * WL.b * (SL - WL.b) - WR.a * WR.b * (SR - WR.b))
+                  / (WL.a * (SL - WL.b) - WR.a * (SR - WR.b));
+    const bool left = (0.0 <= SL) || (0.0 <= S_star);
+    const Q4& U = left ? UL : UR;
+    const Q4& W = left ? WL : WR;
+    const double S = left ? SL : SR;
+    Q4 F = flux_x(U, W);
+    if (0.0 <= SL || !(left || 0.0 <= SR)) return F;   // pure upwind: F(UL) if 0<=SL, F(UR) if SR<0
+    double factor = W.a * (S - W.b) / (S - S_star);
+    Q4 st{factor, factor * S_star, factor * W.c,
+          factor * (U.d / W.a + (S_star - W.b) * (S_star + W.d / (W.a * (S - W.b))))};
+    return Q4{F.a + S * (st.a - U.a), F.b + S * (st.b - U.b), F.c + S * (st.c - U.c), F.d + S * (st.d - U.d)};
+}
+
+// Flux scheme chosen at compile time (one kernel instance per scheme).
+template <int FLUX>
+__device__ __forceinline__ Q4 face_flux(const Q4& UL, const Q4& UR) {
+    if constexpr (FLUX == FLUX_HLLC) return hllc_flux(UL, UR);
+    else return rusanov_flux(UL, UR);
+}
+
+// state2d.hpp:39
+__device__ __forceinline__ Q4 swap_xy(const Q4& U) { return Q4{U.a, U.c, U.b, U.d}; }
+
+// Ghost-cell source index for column/row g of an axis of n physical cells (grid2d.hpp:43-66):
+// periodic ghosts copy the opposite end (modulo n), transmissive ghosts copy the nearest physical cell.
+// Any g is mapped to a valid index, so tiles that overhang the grid read in-bounds memory.
+__device__ __forceinline__ int bc_index(int g, int n, int bc) {
+    if (bc == BC_PERIODIC) {
+        int m = g % n;
+        return m < 0 ? m + n : m;
+    }
+    return g < 0 ? 0 : (g >= n ? n - 1 : g);
+}
+
+}  // namespace fv

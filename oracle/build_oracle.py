@@ -1,0 +1,62 @@
+"""Build recipe for the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+  python oracle/build_oracle.py            # builds what it can
+
+1. oracle/libfvoracle.so  -- the plain-C restatement (oracle/fv_oracle.c), always built.
+2. oracle/_ref/libfvref.so -- oracle/ref_harness.cpp compiled against the reference's own solver
+   headers where they lie (REF_SRC below, read-only), plus the reference's three C++ unit-test
+   programs (test_riemann2d, test_grid2d, test_solver2d) built from their sources into oracle/_ref/.
+   Skipped when the reference tree is absent (the prebuilt files travel with the repo snapshot).
+
+Both are built WITHOUT floating-point contraction (-ffp-contract=off) and without -march, which is
+what makes them bit-identical to each other and to the GPU parity build (nvcc --fmad=false).
+"""
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REF_SRC = Path("/root/reference/solver/src")
+REF_OUT = HERE / "_ref"
+
+CFLAGS = ["-O3", "-fopenmp", "-ffp-contract=off", "-fPIC"]
+
+
+def _run(cmd):
+    subprocess.run(cmd, check=True)
+
+
+def build_oracle(force=False):
+    out = HERE / "libfvoracle.so"
+    src = HERE / "fv_oracle.c"
+    if force or not out.exists() or out.stat().st_mtime < src.stat().st_mtime:
+        _run(["gcc", "-std=c11", *CFLAGS, "-shared", str(src), "-o", str(out), "-lm"])
+    return out
+
+
+def build_ref(force=False):
+    """Returns the path of libfvref.so, or None when the reference sources are not present."""
+    out = REF_OUT / "libfvref.so"
+    if not REF_SRC.is_dir():
+        return out if out.exists() else None
+    REF_OUT.mkdir(exist_ok=True)
+    harness = HERE / "ref_harness.cpp"
+    if force or not out.exists() or out.stat().st_mtime < harness.stat().st_mtime:
+        _run(["g++", "-std=gnu++17", *CFLAGS, "-shared", f"-I{REF_SRC}", str(harness), "-o", str(out)])
+    for t in ("test_riemann2d", "test_grid2d", "test_solver2d"):
+        exe = REF_OUT / t
+        if force or not exe.exists():
+            _run(["g++", "-std=gnu++17", "-O3", "-fopenmp", "-ffp-contract=off", f"-I{REF_SRC}",
+                  str(REF_SRC / f"{t}.cpp"), "-o", str(exe)])
+    return out
+
+
+def build(force=False):
+    build_oracle(force)
+    build_ref(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)
+    print("oracle built:", HERE / "libfvoracle.so", "| reference:", REF_OUT / "libfvref.so")

@@ -1,0 +1,34 @@
+import importlib
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def fvpkg():
+    return importlib.import_module("neural-pde-surrogate_b200")
+
+
+@pytest.fixture(scope="session")
+def oracle_mod():
+    from oracle import build_oracle
+    build_oracle.build_oracle()
+    from oracle import oracle
+    return oracle
+
+
+@pytest.fixture(scope="session")
+def cuda_ok():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test collected on a machine without a CUDA device")
+    return True

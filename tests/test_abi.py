@@ -1,0 +1,69 @@
+"""C-ABI checks that need no GPU: every library loads and exports every symbol its header in
+include/ declares; argument validation fails cleanly (no compute calls are made here)."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+PKG = ROOT / "neural-pde-surrogate_b200"
+
+# header -> shared library that implements it
+LIBS = {"fv.h": "libfv.so"}
+
+
+def declared(header):
+    text = (ROOT / "include" / header).read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w ]*?[\s\*]+(\w+)\s*\(", text, flags=re.M)))
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    import importlib
+    importlib.import_module("neural-pde-surrogate_b200.build").build()
+
+
+@pytest.mark.parametrize("header,lib", sorted(LIBS.items()))
+def test_library_exports_every_declared_symbol(header, lib):
+    path = PKG / lib
+    assert path.exists(), f"{lib} not built"
+    C.CDLL(str(path))
+    names = declared(header)
+    assert len(names) >= 5
+    out = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True, text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    missing = [n for n in names if n not in exported]
+    assert not missing, f"{lib} does not export {missing}"
+
+
+def test_fv_argument_validation_without_gpu(fvpkg):
+    L = fvpkg.lib()
+    h = C.c_void_p()
+    assert L.fv_create(0, 8, 0.0, 1.0, 0.0, 1.0, 1, 1, 1, 3, 0.5, None, C.byref(h)) == 1
+    assert b"positive" in L.fv_last_error()
+    assert L.fv_create(8, 8, 0.0, 1.0, 0.0, 1.0, 1, 1, 7, 3, 0.5, None, C.byref(h)) == 1
+    assert L.fv_create(8, 8, 0.0, 1.0, 0.0, 1.0, 1, 1, 1, 3, -0.5, None, C.byref(h)) == 1
+    assert L.fv_create(8, 8, 0.0, 1.0, 0.0, 1.0, 1, 1, 1, 3, 0.5, None, None) == 1
+    assert L.fv_step(None, 0.1) == 1
+    assert L.fv_version().startswith(b"fv-b200")
+
+
+def test_python_mirror_rejects_unknown_names(fvpkg):
+    g = fvpkg.make_grid(8, 8, 0, 1, 0, 1, "periodic", "periodic")
+    with pytest.raises(ValueError, match="Unknown scheme"):
+        fvpkg.Solver(g, "roe", "vanleer")
+    with pytest.raises(ValueError, match="Unknown limiter"):
+        fvpkg.Solver(g, "hllc", "superbee")
+
+
+def test_no_cpu_fallback(fvpkg):
+    """On a machine without a GPU the product path raises; it never computes on the CPU."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    g = fvpkg.make_grid(8, 8, 0, 1, 0, 1, "periodic", "periodic")
+    with pytest.raises(fvpkg.FVError, match="no CUDA device"):
+        fvpkg.Solver(g, "hllc", "vanleer")

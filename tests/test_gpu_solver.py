@@ -1,0 +1,288 @@
+"""Parity of the CUDA solver (libfv through its C-ABI) with the CPU oracle and the reference's golden
+fixtures.  The bar is bit-exact: the parity build uses no FMA contraction, like the reference."""
+import numpy as np
+import pytest
+
+import known_answers as ka
+from cases import bits_equal, cpu_solver, golden_names, gpu_solver, load_golden, max_rel
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+ic = ka.ic
+
+
+@pytest.fixture(autouse=True)
+def _gpu(cuda_ok):
+    pass
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_gpu_matches_golden(name):
+    d = load_golden(name)
+    s = gpu_solver(d["g"], d["flux"], d["limiter"], float(d["cfl"]))
+    s.set_state(d["U0"])
+    assert s.compute_dt() == float(d["dt0"])
+    times, levels, steps = s.run_trajectory(float(d["t_end"]), 0.0, int(d["nout"]), d["save"] or None)
+    assert steps == int(d["steps"])
+    assert bits_equal(times, d["times"])
+    assert bits_equal(s.get_state(), d["U"])
+    for m in d["save"]:
+        assert bits_equal(levels[m], d[f"level_{m}"])
+
+
+def _random_state(rng, nx, ny):
+    rho = 0.5 + rng.random((ny, nx))
+    u = rng.uniform(-1, 1, (ny, nx))
+    v = rng.uniform(-1, 1, (ny, nx))
+    p = 0.3 + rng.random((ny, nx))
+    return ic.to_conserved(rho, u, v, p)
+
+
+SHAPES = [((1, 5), ("periodic", "transmissive")), ((2, 3), ("transmissive", "periodic")),
+          ((37, 21), ("periodic", "periodic")), ((21, 37), ("transmissive", "transmissive")),
+          ((70, 45), ("periodic", "transmissive")), ((32, 16), ("periodic", "periodic")),
+          ((33, 17), ("transmissive", "periodic"))]
+
+
+@pytest.mark.parametrize("flux", ["hllc", "rusanov"])
+@pytest.mark.parametrize("lim", ["none", "unlimited", "minmod", "vanleer"])
+@pytest.mark.parametrize("shape,bcs", SHAPES)
+def test_gpu_bitexact_vs_oracle(flux, lim, shape, bcs):
+    rng = np.random.default_rng(abs(hash((flux, lim, shape))) % 2**32)
+    nx, ny = shape
+    g = dict(nx=nx, ny=ny, x_min=-0.5, x_max=0.5 + 0.1 * nx, y_min=0.0, y_max=0.7, bc_x=bcs[0], bc_y=bcs[1])
+    U0 = _random_state(rng, nx, ny)
+    a = cpu_solver("oracle", g, flux, lim, 0.45)
+    b = gpu_solver(g, flux, lim, 0.45)
+    a.set_state(U0)
+    b.set_state(U0)
+    for _ in range(3):  # the reference interface: compute_dt + step
+        da, db = a.compute_dt(), b.compute_dt()
+        assert da == db
+        a.step(da)
+        b.step(dt=db)
+    assert bits_equal(a.get_state(), b.get_state())
+    a.advance_to(0.04)
+    t, n = b.advance_to(0.04)
+    assert n == a.steps + 3 and t == a.t  # the device count includes the 3 fv_step calls; t does not
+    assert bits_equal(a.get_state(), b.get_state())
+
+
+@pytest.mark.parametrize("n", [64, 256])
+def test_config0_riemann_full_run_bitexact(n):
+    """Four-quadrant Riemann problem, periodic, HLLC + van Leer, CFL 0.5, to t = 0.25."""
+    rho, u, v, p, t_end, _ = ic.sample("riemann", 0, n)
+    U0 = ic.to_conserved(rho, u, v, p)
+    g = dict(nx=n, ny=n, bc_x="periodic", bc_y="periodic")
+    a = cpu_solver("oracle", g, "hllc", "vanleer")
+    b = gpu_solver(g, "hllc", "vanleer")
+    a.set_state(U0)
+    b.set_state(U0)
+    a.advance_to(t_end)
+    t, steps = b.advance_to(t_end)
+    assert steps == a.steps and t == a.t
+    assert bits_equal(a.get_state(), b.get_state())
+
+
+@pytest.mark.parametrize("flux", ["hllc", "rusanov"])
+@pytest.mark.parametrize("lim", ["minmod", "vanleer"])
+def test_config1_blast_trajectory_bitexact(flux, lim):
+    """Blast + bubbles, periodic, every graded flux x limiter, trajectory mode with 20 frames saved at
+    two coarser sizes; checked at 128^2 to t = 0.2 (the full 512^2 run is covered by
+    test_config1_blast_512_properties)."""
+    n = 128
+    rho, u, v, p, t_end, _ = ic.sample("blast", 1, n)
+    U0 = ic.to_conserved(rho, u, v, p)
+    g = dict(nx=n, ny=n, bc_x="periodic", bc_y="periodic")
+    a = cpu_solver("oracle", g, flux, lim)
+    b = gpu_solver(g, flux, lim)
+    a.set_state(U0)
+    b.set_state(U0)
+    ta, la = a.run(t_end, 0.0, 20, (32, 16))
+    tb, lb, steps = b.run_trajectory(t_end, 0.0, 20, (32, 16))
+    assert steps == a.steps
+    assert bits_equal(ta, tb)
+    for m in (32, 16):
+        assert bits_equal(la[m], lb[m])
+    assert bits_equal(a.get_state(), b.get_state())
+
+
+def test_config1_blast_512_first_steps_bitexact():
+    n = 512
+    rho, u, v, p, _, _ = ic.sample("blast", 2, n)
+    U0 = ic.to_conserved(rho, u, v, p)
+    g = dict(nx=n, ny=n, bc_x="periodic", bc_y="periodic")
+    a = cpu_solver("oracle", g, "hllc", "vanleer")
+    b = gpu_solver(g, "hllc", "vanleer")
+    a.set_state(U0)
+    b.set_state(U0)
+    a.advance_to(0.0015)
+    t, steps = b.advance_to(0.0015)
+    assert steps == a.steps and steps >= 10
+    assert bits_equal(a.get_state(), b.get_state())
+    for f in (4, 8):
+        assert bits_equal(a.block_average(f), b.block_average(f))
+
+
+def test_config1_blast_512_properties():
+    """Size-independent properties of the full 512^2 trajectory (tests/check_trajectory.py:44-74 of
+    the reference): frame times, block-average consistency between levels, totals equal across
+    levels and constant in time (periodic), positivity."""
+    n = 512
+    rho, u, v, p, t_end, _ = ic.sample("blast", 0, n)
+    b = gpu_solver(dict(nx=n, ny=n, bc_x="periodic", bc_y="periodic"), "hllc", "vanleer")
+    b.set_primitive(rho, u, v, p)
+    times, lv, steps = b.run_trajectory(t_end, 0.0, 20, (128, 64))
+    assert np.allclose(times, np.linspace(0, t_end, 21), rtol=0, atol=1e-12)
+    f128, f64 = lv[128].astype(np.float64), lv[64].astype(np.float64)
+    ba = f128.reshape(21, 4, 64, 2, 64, 2).mean(axis=(3, 5))
+    assert np.abs(ba - f64).max() / np.abs(f128).max() < 1e-6
+    tot = f128.mean(axis=(-2, -1))
+    assert np.abs(f64.mean(axis=(-2, -1)) - tot).max() / np.abs(tot).max() < 1e-6
+    drift = np.abs(tot - tot[0]).max(axis=0) / np.abs(tot[0]).clip(1e-12)
+    assert drift[0] < 1e-6 and drift[3] < 1e-6
+    U = b.get_state()
+    r = U[..., 0]
+    pr = 0.4 * (U[..., 3] - 0.5 * (U[..., 1] ** 2 + U[..., 2] ** 2) / r)
+    assert (r > 0).all() and (pr > 0).all()
+    # FP64 totals conserved to roundoff
+    U0 = ic.to_conserved(rho, u, v, p)
+    assert abs(U[..., 0].sum() - U0[..., 0].sum()) / U0[..., 0].sum() < 1e-12
+    assert abs(U[..., 3].sum() - U0[..., 3].sum()) / U0[..., 3].sum() < 1e-12
+
+
+def test_known_answers_on_gpu():
+    """test_solver2d.cpp:35-108 on the CUDA path."""
+    mk = lambda g, f, l, c: gpu_solver(g, f, l, c)
+    assert ka.free_stream(mk) < 1e-13
+    r = ka.check_sod(mk)
+    assert r["same_steps"]
+    assert r["rows_identical"] == 0.0 and r["my_zero"] == 0.0 and r["transpose"] == 0.0
+    assert r["mass"] < 1e-13 and r["energy"] < 1e-13
+    rho, p, u = r["plateau"]
+    assert abs(rho - 0.26557) < 1e-3 and abs(p - 0.30313) < 1e-3 and abs(u - 0.92745) < 1e-3
+
+
+def test_riemann_known_answers_on_gpu(fvpkg):
+    """test_riemann2d.cpp:17-47 on the device flux code, and bit-equality with the oracle's fluxes."""
+    rng = np.random.default_rng(5)
+    UL = _random_state(rng, 64, 4).reshape(-1, 4)
+    UR = _random_state(rng, 64, 4).reshape(-1, 4)
+    for scheme in ("hllc", "rusanov"):
+        for face in ("x", "y"):
+            F = fvpkg.riemann_flux(scheme, UL, UR, face)
+            Fo = np.stack([orc.flux(face, scheme, UL[k], UR[k]) for k in range(len(UL))])
+            assert bits_equal(F, Fo)
+    for s in ka.RIEMANN_STATES:
+        L = ic.to_conserved(np.array(s[0]), np.array(s[1]), np.array(0.0), np.array(s[2]))
+        R = ic.to_conserved(np.array(s[3]), np.array(s[4]), np.array(0.0), np.array(s[5]))
+        F2 = fvpkg.riemann_flux("hllc", L[None], R[None])[0]
+        L1 = np.array([s[0], s[0] * s[1], s[2] / (1.4 - 1.0) + 0.5 * s[0] * s[1] * s[1]])
+        R1 = np.array([s[3], s[3] * s[4], s[5] / (1.4 - 1.0) + 0.5 * s[3] * s[4] * s[4]])
+        F1 = orc.hllc_1d(L1, R1)
+        assert ka.close(F2[0], F1[0]) and ka.close(F2[1], F1[1]) and ka.close(F2[3], F1[2]) and ka.close(F2[2], 0.0)
+        Ly = ic.to_conserved(np.array(s[0]), np.array(0.0), np.array(s[1]), np.array(s[2]))
+        Ry = ic.to_conserved(np.array(s[3]), np.array(0.0), np.array(s[4]), np.array(s[5]))
+        Fy = fvpkg.riemann_flux("hllc", Ly[None], Ry[None], "y")[0]
+        assert ka.close(Fy[0], F2[0]) and ka.close(Fy[2], F2[1]) and ka.close(Fy[3], F2[3])
+    U = ic.to_conserved(np.array(1.3), np.array(0.4), np.array(-0.7), np.array(2.1))
+    F = fvpkg.riemann_flux("hllc", U[None], U[None])[0]
+    u = U[1] / U[0]
+    p = (1.4 - 1.0) * (U[3] - 0.5 * U[0] * (u * u + (U[2] / U[0]) ** 2))
+    assert ka.close(F[1], U[1] * u + p) and ka.close(F[2], U[2] * u) and ka.close(F[3], u * (U[3] + p))
+
+
+@pytest.mark.parametrize("bcs", [("transmissive", "transmissive"), ("periodic", "periodic"), ("periodic", "transmissive"),
+                                 ("transmissive", "periodic")])
+@pytest.mark.parametrize("shape", [(5, 3), (1, 1), (2, 7), (40, 33)])
+def test_ghost_map_matches_apply_bcs(fvpkg, bcs, shape):
+    """test_grid2d.cpp:26-63: the device boundary mapping reproduces apply_bcs, corners included."""
+    nx, ny = shape
+    rng = np.random.default_rng(1)
+    U = rng.random((ny, nx, 4))
+    Ug = np.zeros((ny + 4, nx + 4, 4))
+    Ug[2:-2, 2:-2] = U
+    orc.apply_bcs_ghosted(Ug, *bcs)
+    assert bits_equal(fvpkg.fill_ghosts(U, *bcs), Ug)
+
+
+@pytest.mark.parametrize("index", [1, 2, 4])
+def test_nonphysical_detected_like_reference(index, fvpkg):
+    """The first bad cell (row-major) and the step at which compute_dt trips match the oracle; no exit."""
+    rho, u, v, p, _, _ = ic.sample("blast", index, 64)
+    U0 = ic.to_conserved(rho, u, v, p)
+    g = dict(nx=64, ny=64, bc_x="periodic", bc_y="periodic")
+    a = cpu_solver("oracle", g, "hllc", "unlimited")
+    a.set_state(U0)
+    with pytest.raises(orc.NonPhysical) as ea:
+        a.advance_to(0.2)
+    b = gpu_solver(g, "hllc", "unlimited")
+    b.set_state(U0)
+    with pytest.raises(fvpkg.NonPhysicalError) as eb:
+        b.advance_to(0.2)
+    assert (eb.value.i, eb.value.j) == (ea.value.i, ea.value.j)
+    assert eb.value.rho == ea.value.rho and eb.value.p == ea.value.p
+    assert b.time()[1] == a.steps
+    assert bits_equal(b.get_state(), a.get_state())
+    with pytest.raises(fvpkg.NonPhysicalError):
+        b.compute_dt()
+
+
+def test_set_primitive_rejects_nonpositive(fvpkg):
+    g = dict(nx=8, ny=8, bc_x="periodic", bc_y="periodic")
+    b = gpu_solver(g, "hllc", "vanleer")
+    one = np.ones((8, 8))
+    b.set_primitive(one, 0 * one, 0 * one, one)
+    before = b.get_state()
+    p = one.copy()
+    p[3, 4] = -1.0
+    with pytest.raises(fvpkg.FVError, match="non-positive"):
+        b.set_primitive(one, 0 * one, 0 * one, p)
+    assert bits_equal(before, b.get_state())
+    U = ic.to_conserved(one, 0 * one, 0 * one, one)
+    assert bits_equal(before, U)
+
+
+def test_sod_l1_matches_reference_validation():
+    """README.md:40-45 golden L1 density errors at N = 200 (1D, CFL 0.8 in the reference; here the 2D
+    solver at CFL 0.5): same ordering, within 30%."""
+    ref = {("rusanov", "none"): 1.56e-2, ("hllc", "none"): 1.34e-2, ("hllc", "minmod"): 4.46e-3,
+           ("hllc", "vanleer"): 3.38e-3}
+    got = {}
+    for (flux, lim), val in ref.items():
+        g, t_end, U0 = ic.test_problem("sod_x", 200)
+        s = gpu_solver(g, flux, lim)
+        s.set_state(U0)
+        s.advance_to(t_end)
+        got[(flux, lim)] = ka.sod_l1(s.get_state(), 200)
+        assert abs(got[(flux, lim)] - val) / val < 0.3, (flux, lim, got[(flux, lim)], val)
+    vals = [got[k] for k in ref]
+    assert vals == sorted(vals, reverse=True)
+
+
+def test_sine2d_second_order_with_vanleer():
+    """README.md:50-54: 2D diagonal advection, van Leer order ~2.00 at N up to 256^2."""
+    errs = []
+    for n in (64, 128, 256):
+        g, t_end, U0 = ic.test_problem("sine2d", n)
+        s = gpu_solver(g, "hllc", "vanleer")
+        s.set_state(U0)
+        t, _ = s.advance_to(t_end)
+        x = ic.cell_centres(n)
+        X, Y = np.meshgrid(x, x)
+        exact = 1.0 + 0.2 * np.sin(2 * np.pi * (X + Y - 2 * t))
+        errs.append(np.abs(s.get_state()[..., 0] - exact).sum() / n / n)
+    order = np.log2(errs[-2] / errs[-1])
+    assert 1.8 < order < 2.2, (errs, order)
+
+
+def test_lax_liu3_symmetric_about_diagonal():
+    """README.md:64: Lax-Liu configuration 3 is symmetric about x = y (3e-14 in the reference)."""
+    g, _, U0 = ic.test_problem("lax_liu3", 128)
+    s = gpu_solver(g, "hllc", "vanleer")
+    s.set_state(U0)
+    s.advance_to(0.1)
+    U = s.get_state()
+    asym = max(np.abs(U[..., 0] - U[..., 0].T).max(), np.abs(U[..., 1] - U[..., 2].T).max(),
+               np.abs(U[..., 3] - U[..., 3].T).max())
+    assert asym < 1e-12
