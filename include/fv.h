@@ -122,11 +122,27 @@ int fv_riemann_flux(int flux, int y_face, int n, const double* UL, const double*
  * stored by the solver itself).  Ug: host array of (ny+4)*(nx+4)*4 doubles. */
 int fv_fill_ghosts(int nx, int ny, int bc_x, int bc_y, const double* U, double* Ug);
 
+/* Tile shapes.  The stage kernels exist for several CTA tile shapes (fv_tile_variant enumerates
+ * them: tile width, height, threads); all give bit-identical results.  A handle picks the fastest
+ * for its grid by timing each on a copy of its state the first time it steps (the autotuner; the
+ * choice is cached per device, grid size, flux and limiter for the process).  FV_TILE=<index> in
+ * the environment fixes the shape instead, FV_AUTOTUNE=0 keeps the default.  fv_autotune re-times
+ * now (steps per variant, <= 0 for the default) and returns the chosen index. */
+int fv_autotune(fv_solver* s, int steps, int* variant);
+int fv_set_tile(fv_solver* s, int variant);
+int fv_get_tile(fv_solver* s, int* variant);
+int fv_tile_variant(int variant, int* tx, int* ty, int* threads);
+
 /* Kernel timing (the reference's --profile, solver2d.hpp:29-52, main2d.cpp:261): while enabled,
  * CUDA events bracket every stage-kernel launch of the handle; fv_profile_read returns the mean
  * duration in ms of stage-1 and stage-2 launches and the number of steps timed since enabling. */
 int fv_profile(fv_solver* s, int enable);
 int fv_profile_read(fv_solver* s, double* ms_stage1, double* ms_stage2, long long* steps_timed);
+
+/* Measured FP64 FMA throughput of the current device (DFMA per second, one FMA = 2 flops): the
+ * denominator of the FP64-pipe roofline the stage kernels are reported against.  No reference
+ * counterpart (the reference has no GPU code). */
+int fv_fp64_peak(double* dfma_per_second);
 
 /* Number of kernels the handle has launched since it was created. */
 int fv_launch_count(fv_solver* s, long long* launches);

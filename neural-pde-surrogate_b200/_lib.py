@@ -55,6 +55,11 @@ _PROTOS = {
     "fv_profile": [_P, _I],
     "fv_profile_read": [_P, _DP, _DP, _LLP],
     "fv_launch_count": [_P, _LLP],
+    "fv_fp64_peak": [_DP],
+    "fv_autotune": [_P, _I, C.POINTER(_I)],
+    "fv_set_tile": [_P, _I],
+    "fv_get_tile": [_P, C.POINTER(_I)],
+    "fv_tile_variant": [_I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
 }
 
 _lib = None

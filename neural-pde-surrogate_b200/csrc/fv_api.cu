@@ -7,8 +7,12 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fv.h"
@@ -38,31 +42,47 @@ int set_error(int code, const char* fmt, ...) {
                              __LINE__);                                                                \
     } while (0)
 
-using StageFn = void (*)(StageArgs);
+using StageFn = void (*)(GridDesc);
 
-template <int F, int L>
-void pick_stage(StageFn* s1, StageFn* s2) {
-    *s1 = stage_kernel<F, L, 1>;
-    *s2 = stage_kernel<F, L, 2>;
-}
+// Tile shapes the stage kernels are instantiated for.  All give bit-identical results; the
+// autotuner (fv_autotune) picks the fastest for a grid.  MINB = CTAs per SM the launch bounds ask
+// for: NT * MINB = 1024 threads (32 warps) per SM, which caps registers at 64 per thread.
+struct TileVariant {
+    int tx, ty, nt;
+    size_t smem;
+    StageFn s1[2][4], s2[2][4];  // [flux][limiter]
+};
 
-void stage_fns(int flux, int lim, StageFn* s1, StageFn* s2) {
-    if (flux == FLUX_HLLC) {
-        switch (lim) {
-        case LIM_NONE: pick_stage<FLUX_HLLC, LIM_NONE>(s1, s2); break;
-        case LIM_UNLIMITED: pick_stage<FLUX_HLLC, LIM_UNLIMITED>(s1, s2); break;
-        case LIM_MINMOD: pick_stage<FLUX_HLLC, LIM_MINMOD>(s1, s2); break;
-        default: pick_stage<FLUX_HLLC, LIM_VANLEER>(s1, s2); break;
-        }
-    } else {
-        switch (lim) {
-        case LIM_NONE: pick_stage<FLUX_RUSANOV, LIM_NONE>(s1, s2); break;
-        case LIM_UNLIMITED: pick_stage<FLUX_RUSANOV, LIM_UNLIMITED>(s1, s2); break;
-        case LIM_MINMOD: pick_stage<FLUX_RUSANOV, LIM_MINMOD>(s1, s2); break;
-        default: pick_stage<FLUX_RUSANOV, LIM_VANLEER>(s1, s2); break;
-        }
+template <int TX, int TY, int NT, int MINB>
+struct VariantMaker {
+    template <int F, int L>
+    static void one(TileVariant& v) {
+        v.s1[F][L] = stage_kernel<F, L, 1, TX, TY, NT, MINB>;
+        v.s2[F][L] = stage_kernel<F, L, 2, TX, TY, NT, MINB>;
     }
+    static TileVariant make() {
+        TileVariant v{TX, TY, NT, sizeof(TileSmem<TX, TY>), {}, {}};
+        one<0, 0>(v); one<0, 1>(v); one<0, 2>(v); one<0, 3>(v);
+        one<1, 0>(v); one<1, 1>(v); one<1, 2>(v); one<1, 3>(v);
+        return v;
+    }
+};
+
+const std::vector<TileVariant>& variants() {
+    static const std::vector<TileVariant> v = {
+        VariantMaker<32, 8, 256, 4>::make(),   // 0: default
+        VariantMaker<32, 16, 512, 2>::make(),  // 1
+        VariantMaker<16, 16, 256, 4>::make(),  // 2
+        VariantMaker<64, 8, 512, 2>::make(),   // 3
+        VariantMaker<32, 4, 128, 7>::make(),   // 4
+        VariantMaker<16, 16, 288, 3>::make(),  // 5: 544 faces over 288 threads -> < 2 rounds
+    };
+    return v;
 }
+
+// Autotuned choice per (device, nx, ny, flux, limiter), shared by all handles of the process.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
 
 }  // namespace
 
@@ -74,6 +94,8 @@ struct fv_solver {
     bool own_stream = false;
     Q4* U = nullptr;
     Q4* U1 = nullptr;
+    Q4* W = nullptr;   // to_primitive(U), kept current by every kernel that writes U
+    Q4* W1 = nullptr;  // to_primitive(U1)
     FvCtrl* ctrl = nullptr;
     FvCtrl* h_ctrl = nullptr;  // pinned mirror
     int* d_count = nullptr;
@@ -81,8 +103,8 @@ struct fv_solver {
     double* d_prim = nullptr;  // staging for fv_set_primitive (4 * n doubles), allocated on first use
     float* d_avg = nullptr;
     size_t d_avg_cap = 0;
-    StageFn s1 = nullptr, s2 = nullptr;
-    dim3 grid;
+    int variant = 0;          // tile shape (index into variants())
+    bool tuned = false;       // variant chosen by the autotuner or fixed by fv_set_tile
     bool has_state = false;
     long long launches = 0;  // kernels launched by this handle
     // kernel timing (fv_profile): a ring of event triples bracketing stage 1 and stage 2
@@ -94,6 +116,15 @@ struct fv_solver {
     long long timed = 0;
 
     size_t ncell() const { return size_t(nx) * ny; }
+    GridDesc desc() const {
+        GridDesc g{};
+        g.U = U; g.U1 = U1; g.W = W; g.W1 = W1;
+        g.nx = nx; g.ny = ny; g.bc_x = bc_x; g.bc_y = bc_y;
+        g.dx = dx; g.dy = dy; g.cfl = cfl;
+        g.cx = 1.0 / dx; g.cy = 1.0 / dy;  // (1.0 / g.dx) of solver2d.hpp:149-150
+        g.ctrl = ctrl;
+        return g;
+    }
 };
 
 namespace {
@@ -112,14 +143,39 @@ int retire_oldest(fv_solver* s) {
     return FV_OK;
 }
 
+// Enqueues stage 1 and stage 2 of one step of grid g with tile variant v.
+int enqueue_step(const GridDesc& g, int v, int flux, int lim, cudaStream_t st, cudaEvent_t* ev) {
+    const TileVariant& tv = variants()[v];
+    const dim3 grid((g.nx + tv.tx - 1) / tv.tx, (g.ny + tv.ty - 1) / tv.ty);
+    if (ev) FV_CUDA(cudaEventRecord(ev[0], st));
+    tv.s1[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g);
+    if (ev) FV_CUDA(cudaEventRecord(ev[1], st));
+    tv.s2[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g);
+    if (ev) FV_CUDA(cudaEventRecord(ev[2], st));
+    FV_CUDA(cudaGetLastError());
+    return FV_OK;
+}
+
+int prepare_variants(int flux, int lim) {
+    static std::mutex mu;
+    static bool done[2][4] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[flux][lim]) return FV_OK;
+    for (const TileVariant& v : variants()) {
+        for (StageFn f : {v.s1[flux][lim], v.s2[flux][lim]})
+            FV_CUDA(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem));
+    }
+    done[flux][lim] = true;
+    return FV_OK;
+}
+
+int autotune(fv_solver* s, int steps, int* chosen);
+
 int launch_step(fv_solver* s) {
-    StageArgs a1{};
-    a1.Uin = s->U; a1.Ubase = s->U; a1.Uout = s->U1;
-    a1.nx = s->nx; a1.ny = s->ny; a1.bc_x = s->bc_x; a1.bc_y = s->bc_y;
-    a1.cx = 1.0 / s->dx; a1.cy = 1.0 / s->dy; a1.dx = s->dx; a1.dy = s->dy; a1.cfl = s->cfl;
-    a1.ctrl = s->ctrl;
-    StageArgs a2 = a1;
-    a2.Uin = s->U1; a2.Ubase = s->U; a2.Uout = s->U;
+    if (!s->tuned) {
+        int rc = autotune(s, 8, nullptr);
+        if (rc) return rc;
+    }
     cudaEvent_t* ev = nullptr;
     if (s->profiling) {
         if (s->ring_used == fv_solver::kRing) {  // retire the oldest triple before reusing it
@@ -128,15 +184,9 @@ int launch_step(fv_solver* s) {
         }
         ev = s->ev[(s->ring_head + s->ring_used) % fv_solver::kRing];
         s->ring_used++;
-        FV_CUDA(cudaEventRecord(ev[0], s->stream));
     }
-    s->s1<<<s->grid, NT, sizeof(StageSmem), s->stream>>>(a1);
-    if (ev) FV_CUDA(cudaEventRecord(ev[1], s->stream));
-    s->s2<<<s->grid, NT, sizeof(StageSmem), s->stream>>>(a2);
-    if (ev) FV_CUDA(cudaEventRecord(ev[2], s->stream));
     s->launches += 2;
-    FV_CUDA(cudaGetLastError());
-    return FV_OK;
+    return enqueue_step(s->desc(), s->variant, s->flux, s->lim, s->stream, ev);
 }
 
 int read_ctrl(fv_solver* s) {
@@ -163,11 +213,80 @@ int fill_bad(fv_solver* s, int lin, fv_bad_cell* bad) {
 int prime_state(fv_solver* s, double t, bool reset_step) {
     ctrl_reset_kernel<<<1, 1, 0, s->stream>>>(s->ctrl, t, reset_step ? 1 : 0);
     const int n = int(s->ncell());
-    const int blocks = std::max(1, std::min((n + NT - 1) / NT, 148 * 8));
-    wave_speed_kernel<<<blocks, NT, 0, s->stream>>>(s->U, n, s->ctrl);
+    const int blocks = std::max(1, std::min((n + RED_NT - 1) / RED_NT, 148 * 8));
+    wave_speed_kernel<<<blocks, RED_NT, 0, s->stream>>>(s->U, s->W, n, s->ctrl);
     s->launches += 2;
     FV_CUDA(cudaGetLastError());
     s->has_state = true;
+    return FV_OK;
+}
+
+// Times every tile variant on a copy of the current state (fixed dt from the current CFL dt, so the
+// handle's state, time and control block are untouched) and keeps the fastest.
+int autotune(fv_solver* s, int steps, int* chosen) {
+    s->tuned = true;  // also on failure: never retried inside launch_step
+    const auto key = std::make_tuple(s->device, s->nx, s->ny, s->flux, s->lim);
+    if (!chosen) {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            s->variant = it->second;
+            return FV_OK;
+        }
+    }
+    if (!s->has_state) return FV_OK;  // nothing to time on yet: keep the default shape
+    double dt = 1e-6;
+    {
+        int rc = read_ctrl(s);
+        if (rc) return rc;
+        const FvCtrl& c = *s->h_ctrl;
+        double sx, sy;
+        std::memcpy(&sx, &c.sxy[c.step & 1][0], 8);
+        std::memcpy(&sy, &c.sxy[c.step & 1][1], 8);
+        const double d = s->cfl / (sx / s->dx + sy / s->dy);
+        if (d > 0.0 && std::isfinite(d)) dt = d;
+    }
+    const size_t bytes = s->ncell() * sizeof(Q4);
+    Q4* tmp = nullptr;  // copies of U, U1, W, W1
+    FvCtrl* ct = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = FV_OK, best = s->variant;
+    float best_ms = 1e30f;
+    cudaError_t e = cudaMalloc(&tmp, 4 * bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&ct, sizeof(FvCtrl));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const size_t n = s->ncell();
+    for (int v = 0; e == cudaSuccess && v < (int)variants().size(); ++v) {
+        GridDesc g = s->desc();
+        g.U = tmp; g.U1 = tmp + n; g.W = tmp + 2 * n; g.W1 = tmp + 3 * n; g.ctrl = ct;
+        e = cudaMemcpyAsync(g.U, s->U, bytes, cudaMemcpyDeviceToDevice, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(g.W, s->W, bytes, cudaMemcpyDeviceToDevice, s->stream);
+        if (e != cudaSuccess) break;
+        ctrl_reset_kernel<<<1, 1, 0, s->stream>>>(ct, 0.0, 1);
+        ctrl_set_kernel<<<1, 1, 0, s->stream>>>(ct, MODE_FIXED, 0.0, dt);
+        for (int k = 0; k < 2 && rc == FV_OK; ++k) rc = enqueue_step(g, v, s->flux, s->lim, s->stream, nullptr);
+        if (rc) break;
+        if ((e = cudaEventRecord(e0, s->stream)) != cudaSuccess) break;
+        for (int k = 0; k < steps && rc == FV_OK; ++k) rc = enqueue_step(g, v, s->flux, s->lim, s->stream, nullptr);
+        if (rc) break;
+        if ((e = cudaEventRecord(e1, s->stream)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.f;
+        if ((e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
+        s->launches += 2 * (steps + 2) + 2;
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(tmp);
+    cudaFree(ct);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(FV_ERR_CUDA, "fv_autotune: %s", cudaGetErrorString(e));
+    s->variant = best;
+    if (chosen) *chosen = best;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[key] = best;
     return FV_OK;
 }
 
@@ -203,8 +322,6 @@ int fv_create(int nx, int ny, double x_min, double x_max, double y_min, double y
     s->dy = (y_max - y_min) / ny;
     s->cfl = cfl;
     cudaGetDevice(&s->device);
-    stage_fns(flux, limiter, &s->s1, &s->s2);
-    s->grid = dim3((nx + TX - 1) / TX, (ny + TY - 1) / TY);
     int rc = FV_OK;
     auto fail = [&](cudaError_t e, const char* what) {
         rc = set_error(FV_ERR_CUDA, "fv_create: %s: %s", what, cudaGetErrorString(e));
@@ -219,18 +336,27 @@ int fv_create(int nx, int ny, double x_min, double x_max, double y_min, double y
     }
     if (rc == FV_OK && (e = cudaMalloc(&s->U, s->ncell() * sizeof(Q4))) != cudaSuccess) fail(e, "state");
     if (rc == FV_OK && (e = cudaMalloc(&s->U1, s->ncell() * sizeof(Q4))) != cudaSuccess) fail(e, "stage state");
+    if (rc == FV_OK && (e = cudaMalloc(&s->W, s->ncell() * sizeof(Q4))) != cudaSuccess) fail(e, "primitives");
+    if (rc == FV_OK && (e = cudaMalloc(&s->W1, s->ncell() * sizeof(Q4))) != cudaSuccess) fail(e, "stage primitives");
     if (rc == FV_OK && (e = cudaMalloc(&s->ctrl, sizeof(FvCtrl))) != cudaSuccess) fail(e, "control block");
     if (rc == FV_OK && (e = cudaMalloc(&s->d_count, sizeof(int))) != cudaSuccess) fail(e, "counter");
     if (rc == FV_OK && (e = cudaMallocHost(&s->h_ctrl, sizeof(FvCtrl))) != cudaSuccess) fail(e, "pinned control");
     if (rc == FV_OK && (e = cudaMallocHost(&s->h_count, sizeof(int))) != cudaSuccess) fail(e, "pinned counter");
     if (rc == FV_OK && (e = cudaMemsetAsync(s->ctrl, 0, sizeof(FvCtrl), s->stream)) != cudaSuccess) fail(e, "memset");
+    if (rc == FV_OK) rc = prepare_variants(flux, limiter);
     if (rc == FV_OK) {
-        for (StageFn f : {s->s1, s->s2}) {
-            if ((e = cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sizeof(StageSmem))) != cudaSuccess) {
-                fail(e, "smem attribute");
-                break;
-            }
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find({s->device, nx, ny, flux, limiter});
+        const char* env = getenv("FV_TILE");
+        const char* at = getenv("FV_AUTOTUNE");
+        if (env && atoi(env) >= 0 && atoi(env) < (int)variants().size()) {  // fixed tile shape
+            s->variant = atoi(env);
+            s->tuned = true;
+        } else if (it != g_tuned.end()) {
+            s->variant = it->second;
+            s->tuned = true;
+        } else if (at && atoi(at) == 0) {
+            s->tuned = true;  // keep the default variant
         }
     }
     if (rc != FV_OK) {
@@ -249,6 +375,8 @@ int fv_destroy(fv_solver* s) {
             if (e) cudaEventDestroy(e);
     cudaFree(s->U);
     cudaFree(s->U1);
+    cudaFree(s->W);
+    cudaFree(s->W1);
     cudaFree(s->ctrl);
     cudaFree(s->d_count);
     cudaFree(s->d_prim);
@@ -366,15 +494,14 @@ int fv_advance_to(fv_solver* s, double t_next, double* t_out, long long* steps_o
         if (c.status) break;
         const double t = c.t[c.step & 1];
         if (!(t < t_next)) break;
-        double dt_est = c.dt;
-        if (!(dt_est > 0.0)) {
-            double sx, sy;
-            std::memcpy(&sx, &c.sxy[c.step & 1][0], 8);
-            std::memcpy(&sy, &c.sxy[c.step & 1][1], 8);
-            dt_est = s->cfl / (sx / s->dx + sy / s->dy);
-        }
+        // CFL dt of the current state (the last dt of a frame is clamped to land on it, so it is
+        // useless as an estimate); the remaining steps are estimated from it without overshoot.
+        double sx, sy;
+        std::memcpy(&sx, &c.sxy[c.step & 1][0], 8);
+        std::memcpy(&sy, &c.sxy[c.step & 1][1], 8);
+        const double dt_est = s->cfl / (sx / s->dx + sy / s->dy);
         double est = (dt_est > 0.0) ? std::ceil((t_next - t) / dt_est) : 1.0;
-        int batch = (int)std::min<double>(std::max(est, 1.0) + 1.0, (double)kMaxBatch);
+        int batch = (int)std::min<double>(std::max(est, 1.0), (double)kMaxBatch);
         for (int k = 0; k < batch; ++k)
             if ((rc = launch_step(s))) return rc;
         if ((rc = read_ctrl(s))) return rc;
@@ -497,6 +624,38 @@ int fv_fill_ghosts(int nx, int ny, int bc_x, int bc_y, const double* U, double* 
     if (e == cudaSuccess) e = cudaMemcpy(Ug, d + n_in, n_out * sizeof(Q4), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) return set_error(FV_ERR_CUDA, "fv_fill_ghosts: %s", cudaGetErrorString(e));
+    return FV_OK;
+}
+
+int fv_autotune(fv_solver* s, int steps, int* variant) {
+    if (!s) return set_error(FV_ERR_ARG, "fv_autotune: NULL handle");
+    if (!s->has_state) return set_error(FV_ERR_STATE, "fv_autotune: no state set");
+    int v = 0;
+    int rc = autotune(s, steps > 0 ? steps : 8, &v);
+    if (rc == FV_OK && variant) *variant = v;
+    return rc;
+}
+
+int fv_set_tile(fv_solver* s, int variant) {
+    if (!s) return set_error(FV_ERR_ARG, "fv_set_tile: NULL handle");
+    if (variant < 0 || variant >= (int)variants().size()) return set_error(FV_ERR_ARG, "fv_set_tile: no variant %d", variant);
+    s->variant = variant;
+    s->tuned = true;
+    return FV_OK;
+}
+
+int fv_get_tile(fv_solver* s, int* variant) {
+    if (!s || !variant) return set_error(FV_ERR_ARG, "fv_get_tile: NULL argument");
+    *variant = s->variant;
+    return FV_OK;
+}
+
+int fv_tile_variant(int variant, int* tx, int* ty, int* threads) {
+    if (variant < 0 || variant >= (int)variants().size()) return set_error(FV_ERR_ARG, "fv_tile_variant: no variant %d", variant);
+    const TileVariant& v = variants()[variant];
+    if (tx) *tx = v.tx;
+    if (ty) *ty = v.ty;
+    if (threads) *threads = v.nt;
     return FV_OK;
 }
 

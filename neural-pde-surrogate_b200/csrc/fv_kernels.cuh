@@ -1,7 +1,7 @@
 // Kernels of the finite-volume step (one fused kernel per SSP-RK2 stage), the on-device time
 // control, the wave-speed / positivity reduction and the trajectory block average.
 //
-// Stage kernel (one CTA per TX x TY tile of interior cells, NT threads):
+// Stage kernel, one CTA per TX x TY tile of interior cells (NT threads, one per cell):
 //   P1  load the tile plus a 2-cell halo of the stage input (ghosts resolved by bc_index: periodic
 //       wrap or transmissive clamp, grid2d.hpp:43-66), convert to primitives      -> smem W
 //   P2  limited slopes in x (cells -1..TX) and y (rows -1..TY)  (solver2d.hpp:142-143,159-162)
@@ -11,35 +11,47 @@
 //       (solver2d.hpp:141,149-150,176-177), then the stage update (solver2d.hpp:92 / :100).
 //       Stage 2 also reduces the next step's CFL wave speeds and the first non-physical cell
 //       (compute_dt, solver2d.hpp:67-83) into the control block: dt never leaves the device.
+// Shared memory is structure-of-arrays (one plane per variable) so that a warp reading 32
+// consecutive cells touches 32 consecutive doubles: no bank conflicts.
+// Every face flux is computed from the same inputs in the same order whatever the tile shape, so all
+// tile shapes give bit-identical results; the shape is a tuning choice (fv_autotune).
 #pragma once
 #include <climits>
 #include "fv_physics.cuh"
 
+// Phase marker inside tile_body (no-op unless a build defines it, e.g. to record clock64()).
+#ifndef FV_PHASE_MARK
+#define FV_PHASE_MARK(k)
+#endif
+
 namespace fv {
 
-constexpr int TX = 32, TY = 16, NT = 256;
-constexpr int HX = TX + 4, HY = TY + 4;  // loaded tile with its 2-cell halo
-constexpr int SXW = TX + 2;              // x-slopes per row: cells -1..TX
-constexpr int SYH = TY + 2;              // y-slope rows: -1..TY
-constexpr int FXW = TX + 1;              // x-faces per row
-constexpr int GYH = TY + 1;              // y-face rows
-constexpr int NFX = TY * FXW, NFY = GYH * TX;
-
-struct StageSmem {
-    Q4 W[HY][HX];
-    Q4 dWx[TY][SXW];
-    Q4 dWy[SYH][TX];
-    Q4 F[TY][FXW];
-    Q4 G[GYH][TX];
+template <int TX_, int TY_>
+struct TileSmem {
+    static constexpr int TX = TX_, TY = TY_, HX = TX + 4, HY = TY + 4;
+    double W[4][HY][HX];        // primitives of the tile + 2-cell halo
+    double dX[4][TY][TX + 2];   // x-slopes of cells -1..TX
+    double dY[4][TY + 2][TX];   // y-slopes of rows -1..TY
+    double F[4][TY][TX + 1];    // x-face fluxes
+    double G[4][TY + 1][TX];    // y-face fluxes
 };
+
+template <int R, int Cc>
+__device__ __forceinline__ Q4 lds(const double (&a)[4][R][Cc], int r, int c) {
+    return Q4{a[0][r][c], a[1][r][c], a[2][r][c], a[3][r][c]};
+}
+template <int R, int Cc>
+__device__ __forceinline__ void sts(double (&a)[4][R][Cc], int r, int c, const Q4& q) {
+    a[0][r][c] = q.a; a[1][r][c] = q.b; a[2][r][c] = q.c; a[3][r][c] = q.d;
+}
 
 enum : int { MODE_LOOP = 0, MODE_FIXED = 1 };
 
 // Control block of one grid (device memory).  Fields are double-buffered by step parity so that a
 // kernel never reads a field another CTA of the same kernel writes:
-//   stage 1 reads step, t[par], sxy[par], bad[par] and (CTA 0 only) writes dt, t[par^1], par2, run2
-//   and resets sxy[par^1], bad[par^1]; stage 2 reads dt, par2, run2, accumulates into sxy[par2],
-//   bad[par2] and (CTA 0 only) increments step.
+//   stage 1 reads step, t[par], sxy[par], bad[par] and (leader CTA only) writes dt, t[par^1],
+//   par2, run2 and resets sxy[par^1], bad[par^1]; stage 2 reads dt, par2, run2, accumulates into
+//   sxy[par2], bad[par2] and (leader only) increments step.
 struct FvCtrl {
     unsigned long long sxy[2][2];  // bit patterns of the non-negative max wave speeds (x, y)
     int bad[2];                    // min row-major index of a non-physical cell, INT_MAX if none
@@ -55,13 +67,18 @@ struct FvCtrl {
     int pad_;
 };
 
-struct StageArgs {
-    const Q4* Uin;    // state whose RHS is evaluated: U (stage 1) or U1 (stage 2)
-    const Q4* Ubase;  // U (stage 2)
-    Q4* Uout;         // U1 (stage 1) or U in place (stage 2)
+// One grid as the stage kernels see it.  W and W1 hold to_primitive(U) and to_primitive(U1): each
+// stage writes the primitives of the state it produces (it needs them anyway for the wave speeds or
+// costs one conversion per cell), so the next stage loads its tile + halo as primitives instead of
+// converting 1.4-1.7 cells per cell.  The conversion is deterministic, so the bits are unchanged.
+struct GridDesc {
+    Q4* U;            // state (stage 2 writes it in place)
+    Q4* U1;           // intermediate RK stage
+    Q4* W;            // to_primitive(U)
+    Q4* W1;           // to_primitive(U1)
     int nx, ny, bc_x, bc_y;
-    double cx, cy;    // 1.0/dx and 1.0/dy, as the reference writes (1.0 / g.dx)
     double dx, dy, cfl;
+    double cx, cy;    // 1.0/dx and 1.0/dy, as the reference writes (1.0 / g.dx)
     FvCtrl* ctrl;
 };
 
@@ -76,9 +93,9 @@ __device__ __forceinline__ int warp_min_int(int v) {
     return v;
 }
 
-// compute_dt's per-cell work (solver2d.hpp:74-78): non-physical cells are recorded, not maxed.
-__device__ __forceinline__ void wave_speed_cell(const Q4& U, int lin, double& sx, double& sy, int& bad) {
-    Q4 W = to_primitive(U);
+// compute_dt's per-cell work (solver2d.hpp:74-78) on W = to_primitive(U): non-physical cells are
+// recorded, not maxed.
+__device__ __forceinline__ void wave_speed_cell(const Q4& W, int lin, double& sx, double& sy, int& bad) {
     if (!(W.a > 0.0) || !(W.d > 0.0)) {
         bad = min(bad, lin);
         return;
@@ -90,9 +107,11 @@ __device__ __forceinline__ void wave_speed_cell(const Q4& U, int lin, double& sx
 
 // Block-wide reduction of (sx, sy, bad) into ctrl slot `par` (atomics; max/min are order-free, so
 // the result is deterministic).  Must be called by all NT threads.
+template <int NT>
 __device__ __forceinline__ void reduce_wave_speeds(double sx, double sy, int bad, FvCtrl* c, int par) {
-    __shared__ double rsx[NT / 32], rsy[NT / 32];
-    __shared__ int rbad[NT / 32];
+    constexpr int NW = NT / 32;
+    __shared__ double rsx[NW], rsy[NW];
+    __shared__ int rbad[NW];
     sx = warp_max(sx);
     sy = warp_max(sy);
     bad = warp_min_int(bad);
@@ -100,9 +119,9 @@ __device__ __forceinline__ void reduce_wave_speeds(double sx, double sy, int bad
     if (l == 0) { rsx[w] = sx; rsy[w] = sy; rbad[w] = bad; }
     __syncthreads();
     if (w == 0) {
-        sx = l < NT / 32 ? rsx[l] : 0.0;
-        sy = l < NT / 32 ? rsy[l] : 0.0;
-        bad = l < NT / 32 ? rbad[l] : INT_MAX;
+        sx = l < NW ? rsx[l] : 0.0;
+        sy = l < NW ? rsy[l] : 0.0;
+        bad = l < NW ? rbad[l] : INT_MAX;
         sx = warp_max(sx);
         sy = warp_max(sy);
         bad = warp_min_int(bad);
@@ -114,124 +133,117 @@ __device__ __forceinline__ void reduce_wave_speeds(double sx, double sy, int bad
     }
 }
 
-template <int FLUX, int LIM, int STAGE>
-__global__ void __launch_bounds__(NT, 2) stage_kernel(StageArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem& s = *reinterpret_cast<StageSmem*>(smem_raw);
-    FvCtrl* c = a.ctrl;
-    const bool cta0 = (blockIdx.x == 0 && blockIdx.y == 0);
-    double dt;
-    int par2 = 0;
-
-    if constexpr (STAGE == 1) {
-        // ---- step control: dt = min(compute_dt(U), t_next - t) (main2d.cpp:238, solver2d.hpp:82) ----
-        const long long step = c->step;
-        const int par = int(step & 1);
-        const double t = c->t[par];
-        bool active = true;
-        if (c->mode == MODE_FIXED) {
-            dt = c->dt_fixed;
-        } else {
-            active = (c->status == 0) && (t < c->t_next);
-            if (active && c->bad[par] != INT_MAX) {
-                active = false;
-                if (cta0 && threadIdx.x == 0) {
-                    c->status = 3;  // FV_ERR_NONPHYSICAL
-                    c->bad_index = c->bad[par];
-                }
-            }
-            dt = 0.0;
-            if (active) {
-                const double sx = __longlong_as_double((long long)c->sxy[par][0]);
-                const double sy = __longlong_as_double((long long)c->sxy[par][1]);
-                dt = smin(a.cfl / (sx / a.dx + sy / a.dy), c->t_next - t);
-            }
-        }
-        if (cta0 && threadIdx.x == 0) {
-            c->run2 = active ? 1 : 0;
-            if (active) {
-                c->dt = dt;
-                // fv_step mirrors Solver::step, which has no notion of time: only the loop advances t
-                c->t[par ^ 1] = (c->mode == MODE_FIXED) ? t : t + dt;
-                c->par2 = par ^ 1;
-                c->sxy[par ^ 1][0] = 0ull;
-                c->sxy[par ^ 1][1] = 0ull;
-                c->bad[par ^ 1] = INT_MAX;
-            }
-        }
-        if (!active) return;
+// Step control of stage 1, run by one thread per CTA: dt = min(compute_dt(U), t_next - t)
+// (main2d.cpp:238, solver2d.hpp:82), or the fixed dt of fv_step.  The leader (one CTA per grid)
+// records it for stage 2 and prepares the next reduction slot.  Returns whether the grid steps.
+__device__ __forceinline__ bool stage1_control(FvCtrl* c, const GridDesc& g, bool leader, double& dt) {
+    const long long step = c->step;
+    const int par = int(step & 1);
+    const double t = c->t[par];
+    bool active = true;
+    dt = 0.0;
+    if (c->mode == MODE_FIXED) {
+        dt = c->dt_fixed;
     } else {
-        if (!c->run2) return;
-        dt = c->dt;
-        par2 = c->par2;
+        active = (c->status == 0) && (t < c->t_next);
+        if (active && c->bad[par] != INT_MAX) {
+            active = false;
+            if (leader) {
+                c->status = 3;  // FV_ERR_NONPHYSICAL
+                c->bad_index = c->bad[par];
+            }
+        }
+        if (active) {
+            const double sx = __longlong_as_double((long long)c->sxy[par][0]);
+            const double sy = __longlong_as_double((long long)c->sxy[par][1]);
+            dt = smin(g.cfl / (sx / g.dx + sy / g.dy), c->t_next - t);
+        }
     }
+    if (leader) {
+        c->run2 = active ? 1 : 0;
+        if (active) {
+            c->dt = dt;
+            // fv_step mirrors Solver::step, which has no notion of time: only the loop advances t
+            c->t[par ^ 1] = (c->mode == MODE_FIXED) ? t : t + dt;
+            c->par2 = par ^ 1;
+            c->sxy[par ^ 1][0] = 0ull;
+            c->sxy[par ^ 1][1] = 0ull;
+            c->bad[par ^ 1] = INT_MAX;
+        }
+    }
+    return active;
+}
 
-    const int nx = a.nx, ny = a.ny;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-    const Q4* __restrict__ Uin = a.Uin;
+// The stage computation of one tile.  STAGE 1: U1 = U + dt L(U).  STAGE 2: U = 0.5 ((U + U1) +
+// dt L(U1)), plus the wave speeds of the new U into (sx, sy, bad).
+template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT>
+__device__ __forceinline__ void tile_body(const GridDesc& g, int i0, int j0, double dt, TileSmem<TX, TY>& s,
+                                          double& sx, double& sy, int& bad) {
+    using S = TileSmem<TX, TY>;
+    constexpr int HX = S::HX, HY = S::HY;
+    constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
+    constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
+    const int nx = g.nx, ny = g.ny;
+    const Q4* __restrict__ Win = (STAGE == 1) ? g.W : g.W1;
 
-    // P1: halo tile -> primitives (solver2d.hpp:133-134 on the ghost-filled array)
+    FV_PHASE_MARK(0);
+    // P1: primitives of the halo tile (solver2d.hpp:133-134 on the ghost-filled array)
     for (int e = threadIdx.x; e < HX * HY; e += NT) {
         const int r = e / HX, col = e - r * HX;
-        const int gi = bc_index(i0 - 2 + col, nx, a.bc_x);
-        const int gj = bc_index(j0 - 2 + r, ny, a.bc_y);
-        st_q4(&s.W[r][col], to_primitive(ldg_q4(Uin + (size_t)gj * nx + gi)));
+        const int gi = bc_index(i0 - 2 + col, nx, g.bc_x);
+        const int gj = bc_index(j0 - 2 + r, ny, g.bc_y);
+        sts(s.W, r, col, ldg_q4(Win + (size_t)gj * nx + gi));
     }
     __syncthreads();
+    FV_PHASE_MARK(1);
 
     // P2: limited slopes
-    for (int e = threadIdx.x; e < TY * SXW + SYH * TX; e += NT) {
-        if (e < TY * SXW) {
-            const int r = e / SXW, k = e - r * SXW;  // cell (k-1, r): W[r+2][k+1]
-            st_q4(&s.dWx[r][k], limited_slope<LIM>(ld_q4(&s.W[r + 2][k]), ld_q4(&s.W[r + 2][k + 1]),
-                                                   ld_q4(&s.W[r + 2][k + 2])));
+    for (int e = threadIdx.x; e < NSX + NSY; e += NT) {
+        if (e < NSX) {
+            const int r = e / (TX + 2), k = e - r * (TX + 2);  // cell (k-1, r) = W[r+2][k+1]
+            sts(s.dX, r, k, limited_slope<LIM>(lds(s.W, r + 2, k), lds(s.W, r + 2, k + 1), lds(s.W, r + 2, k + 2)));
         } else {
-            const int e2 = e - TY * SXW;
-            const int r = e2 / TX, k = e2 - r * TX;  // cell (k, r-1): W[r+1][k+2]
-            st_q4(&s.dWy[r][k], limited_slope<LIM>(ld_q4(&s.W[r][k + 2]), ld_q4(&s.W[r + 1][k + 2]),
-                                                   ld_q4(&s.W[r + 2][k + 2])));
+            const int e2 = e - NSX;
+            const int r = e2 / TX, k = e2 - r * TX;  // cell (k, r-1) = W[r+1][k+2]
+            sts(s.dY, r, k, limited_slope<LIM>(lds(s.W, r, k + 2), lds(s.W, r + 1, k + 2), lds(s.W, r + 2, k + 2)));
         }
     }
     __syncthreads();
+    FV_PHASE_MARK(2);
 
     // P3: face fluxes, flux(to_conserved(edge(W_L, dW_L, +1)), to_conserved(edge(W_R, dW_R, -1)))
     for (int e = threadIdx.x; e < NFX + NFY; e += NT) {
-        const Q4 *wl, *dl, *wr, *dr;
-        Q4* out;
-        bool ydir;
-        if (e < NFX) {  // x-face f of row r, between cells f-1 and f (solver2d.hpp:145-148)
-            const int r = e / FXW, f = e - r * FXW;
-            wl = &s.W[r + 2][f + 1]; dl = &s.dWx[r][f];
-            wr = &s.W[r + 2][f + 2]; dr = &s.dWx[r][f + 1];
-            out = &s.F[r][f];
-            ydir = false;
-        } else {        // y-face g of column k, between rows g-1 and g (solver2d.hpp:165-169)
+        Q4 wl, dl, wr, dr;
+        const bool ydir = e >= NFX;
+        int r, k;
+        if (!ydir) {  // x-face k of row r, between cells k-1 and k (solver2d.hpp:145-148)
+            r = e / (TX + 1); k = e - r * (TX + 1);
+            wl = lds(s.W, r + 2, k + 1); dl = lds(s.dX, r, k);
+            wr = lds(s.W, r + 2, k + 2); dr = lds(s.dX, r, k + 1);
+        } else {      // y-face r of column k, between rows r-1 and r (solver2d.hpp:165-169)
             const int e2 = e - NFX;
-            const int g = e2 / TX, k = e2 - g * TX;
-            wl = &s.W[g + 1][k + 2]; dl = &s.dWy[g][k];
-            wr = &s.W[g + 2][k + 2]; dr = &s.dWy[g + 1][k];
-            out = &s.G[g][k];
-            ydir = true;
+            r = e2 / TX; k = e2 - r * TX;
+            wl = lds(s.W, r + 1, k + 2); dl = lds(s.dY, r, k);
+            wr = lds(s.W, r + 2, k + 2); dr = lds(s.dY, r + 1, k);
         }
-        Q4 UL = to_conserved(edge(ld_q4(wl), ld_q4(dl), +1.0));
-        Q4 UR = to_conserved(edge(ld_q4(wr), ld_q4(dr), -1.0));
+        Q4 UL = to_conserved(edge(wl, dl, +1.0));
+        Q4 UR = to_conserved(edge(wr, dr, -1.0));
         if (ydir) { UL = swap_xy(UL); UR = swap_xy(UR); }
         Q4 F = face_flux<FLUX>(UL, UR);
-        if (ydir) F = swap_xy(F);
-        st_q4(out, F);
+        if (ydir) sts(s.G, r, k, swap_xy(F));
+        else sts(s.F, r, k, F);
     }
     __syncthreads();
+    FV_PHASE_MARK(3);
 
     // P4: divergence + stage update
-    double sx = 0.0, sy = 0.0;
-    int bad = INT_MAX;
-    const double cx = a.cx, cy = a.cy;
+    const double cx = g.cx, cy = g.cy;
     for (int e = threadIdx.x; e < TX * TY; e += NT) {
         const int r = e / TX, k = e - r * TX;
         const int i = i0 + k, j = j0 + r;
         if (i >= nx || j >= ny) continue;
-        const Q4 Fl = ld_q4(&s.F[r][k]), Fr = ld_q4(&s.F[r][k + 1]);
-        const Q4 Gb = ld_q4(&s.G[r][k]), Gt = ld_q4(&s.G[r + 1][k]);
+        const Q4 Fl = lds(s.F, r, k), Fr = lds(s.F, r, k + 1);
+        const Q4 Gb = lds(s.G, r, k), Gt = lds(s.G, r + 1, k);
         Q4 L;
         L.a = (0.0 + cx * Fl.a) - cx * Fr.a;
         L.b = (0.0 + cx * Fl.b) - cx * Fr.b;
@@ -243,31 +255,69 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(StageArgs a) {
         L.d = L.d + cy * Gb.d; L.d = L.d - cy * Gt.d;
         const size_t idx = (size_t)j * nx + i;
         if constexpr (STAGE == 1) {
-            const Q4 u = ldg_q4(Uin + idx);
-            st_q4(a.Uout + idx, Q4{u.a + dt * L.a, u.b + dt * L.b, u.c + dt * L.c, u.d + dt * L.d});
+            const Q4 u = ldg_q4(g.U + idx);
+            const Q4 u1{u.a + dt * L.a, u.b + dt * L.b, u.c + dt * L.c, u.d + dt * L.d};
+            st_q4(g.U1 + idx, u1);
+            st_q4(g.W1 + idx, to_primitive(u1));
         } else {
-            const Q4 u = ld_q4(a.Ubase + idx);
-            const Q4 u1 = ldg_q4(Uin + idx);
+            const Q4 u = ld_q4(g.U + idx);
+            const Q4 u1 = ldg_q4(g.U1 + idx);
             const Q4 un{0.5 * (u.a + u1.a + dt * L.a), 0.5 * (u.b + u1.b + dt * L.b),
                         0.5 * (u.c + u1.c + dt * L.c), 0.5 * (u.d + u1.d + dt * L.d)};
-            st_q4(a.Uout + idx, un);
-            wave_speed_cell(un, (int)idx, sx, sy, bad);
+            const Q4 wn = to_primitive(un);
+            st_q4(g.U + idx, un);
+            st_q4(g.W + idx, wn);
+            wave_speed_cell(wn, (int)idx, sx, sy, bad);
         }
-    }
-    if constexpr (STAGE == 2) {
-        reduce_wave_speeds(sx, sy, bad, c, par2);
-        if (cta0 && threadIdx.x == 0) c->step = c->step + 1;
     }
 }
 
-// Wave speeds / positivity of the current state into slot step&1 (after fv_set_state).
-__global__ void __launch_bounds__(NT) wave_speed_kernel(const Q4* __restrict__ U, int n, FvCtrl* c) {
+// Single-grid stage kernel: grid (ceil(nx/TX), ceil(ny/TY)), one tile per CTA.
+template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(GridDesc g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
+    __shared__ double s_dt;
+    __shared__ int s_go, s_par2;
+    FvCtrl* c = g.ctrl;
+    const bool leader = (blockIdx.x == 0 && blockIdx.y == 0);
+    if (threadIdx.x == 0) {
+        double dt;
+        int go, par2 = 0;
+        if constexpr (STAGE == 1) {
+            go = stage1_control(c, g, leader, dt);
+        } else {
+            go = c->run2;
+            dt = c->dt;
+            par2 = c->par2;
+        }
+        s_go = go; s_dt = dt; s_par2 = par2;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    double sx = 0.0, sy = 0.0;
+    int bad = INT_MAX;
+    tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, blockIdx.x * TX, blockIdx.y * TY, s_dt, s, sx, sy, bad);
+    if constexpr (STAGE == 2) {
+        reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
+        if (leader && threadIdx.x == 0) c->step = c->step + 1;
+    }
+}
+
+// After the state changed from outside the stage kernels: W = to_primitive(U), and the wave speeds /
+// positivity of U into slot step&1.
+constexpr int RED_NT = 256;
+__global__ void __launch_bounds__(RED_NT) wave_speed_kernel(const Q4* __restrict__ U, Q4* __restrict__ W, int n,
+                                                            FvCtrl* c) {
     const int par = int(c->step & 1);
     double sx = 0.0, sy = 0.0;
     int bad = INT_MAX;
-    for (int k = blockIdx.x * NT + threadIdx.x; k < n; k += gridDim.x * NT)
-        wave_speed_cell(ldg_q4(U + k), k, sx, sy, bad);
-    reduce_wave_speeds(sx, sy, bad, c, par);
+    for (int k = blockIdx.x * RED_NT + threadIdx.x; k < n; k += gridDim.x * RED_NT) {
+        const Q4 w = to_primitive(ldg_q4(U + k));
+        st_q4(W + k, w);
+        wave_speed_cell(w, k, sx, sy, bad);
+    }
+    reduce_wave_speeds<RED_NT>(sx, sy, bad, c, par);
 }
 
 __global__ void ctrl_reset_kernel(FvCtrl* c, double t, int reset_step) {

@@ -238,3 +238,32 @@ def launch_count(solver):
     n = C.c_longlong()
     check(lib().fv_launch_count(solver._h, C.byref(n)))
     return n.value
+
+
+def tile_variants():
+    """[(tile width, tile height, threads)] of the stage-kernel tile shapes (fv_tile_variant)."""
+    out = []
+    k = 0
+    while True:
+        tx, ty, nt = C.c_int(), C.c_int(), C.c_int()
+        if lib().fv_tile_variant(k, C.byref(tx), C.byref(ty), C.byref(nt)) != 0:
+            return out
+        out.append((tx.value, ty.value, nt.value))
+        k += 1
+
+
+def set_tile(solver, variant):
+    check(lib().fv_set_tile(solver._h, int(variant)))
+
+
+def get_tile(solver):
+    v = C.c_int()
+    check(lib().fv_get_tile(solver._h, C.byref(v)))
+    return v.value
+
+
+def autotune(solver, steps=8):
+    """Re-time every tile shape on a copy of the solver's state; returns the chosen index."""
+    v = C.c_int()
+    check(lib().fv_autotune(solver._h, int(steps), C.byref(v)))
+    return v.value

@@ -2,6 +2,7 @@
 the reference's own unit programs, bit-for-bit agreement with the reference build on random cases,
 the golden fixtures, and the reference's known answers."""
 import subprocess
+import zlib
 
 import numpy as np
 import pytest
@@ -55,7 +56,7 @@ def _random_case(rng, nx, ny, bcx, bcy):
 @pytest.mark.parametrize("shape,bcs", [((1, 5), ("periodic", "transmissive")), ((2, 3), ("transmissive", "periodic")),
                                        ((37, 21), ("periodic", "periodic")), ((21, 37), ("transmissive", "transmissive"))])
 def test_oracle_bitexact_vs_reference(flux, lim, shape, bcs):
-    rng = np.random.default_rng(hash((flux, lim, shape)) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(repr((flux, lim, shape)).encode()))
     g, U0 = _random_case(rng, shape[0], shape[1], *bcs)
     a = cpu_solver("oracle", g, flux, lim, 0.45)
     b = cpu_solver("ref", g, flux, lim, 0.45)
@@ -67,8 +68,14 @@ def test_oracle_bitexact_vs_reference(flux, lim, shape, bcs):
         a.step(da)
         b.step(db)
     assert bits_equal(a.get_state(), b.get_state())
-    ta, la = a.run(0.05, 0.0, 2, ())
-    tb, lb = b.run(0.05, 0.0, 2, ())
+    outcome = []
+    for s in (a, b):
+        try:
+            s.run(0.05, 0.0, 2, ())
+            outcome.append(None)
+        except orc.NonPhysical as e:  # unlimited slopes may blow up: both must stop at the same cell
+            outcome.append((e.i, e.j))
+    assert outcome[0] == outcome[1]
     assert a.steps == b.steps and bits_equal(a.get_state(), b.get_state())
 
 
