@@ -144,6 +144,19 @@ int fv_profile_read(fv_solver* s, double* ms_stage1, double* ms_stage2, long lon
  * counterpart (the reference has no GPU code). */
 int fv_fp64_peak(double* dfma_per_second);
 
+/* One SSP-RK2 step with a fixed dt (Solver::step semantics, bit-identical to fv_step) on a
+ * caller-owned device state d_U (interior layout above, updated in place), that allocates no device
+ * memory: for callers that cannot call cudaMalloc at that point -- a host running inside another
+ * framework's memory pool, or a driver loop that forbids allocation after start-up.  Its scratch is
+ * a fixed array compiled into the library (about 1.5 MB, held by every GPU that loads the library
+ * until exit), so grids are limited to FV_NOALLOC_MAX_CELLS cells (larger ones return FV_ERR_ARG).
+ * All calls on a device share that scratch: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device sets up the scratch address; make it before
+ * any stream capture.  stream: a cudaStream_t or NULL.  No counterpart in the reference. */
+#define FV_NOALLOC_MAX_CELLS (128 * 128)
+int fv_step_noalloc(int nx, int ny, double x_min, double x_max, double y_min, double y_max, int bc_x, int bc_y,
+                    int flux, int limiter, double* d_U, double dt, void* stream);
+
 /* Number of kernels the handle has launched since it was created. */
 int fv_launch_count(fv_solver* s, long long* launches);
 

@@ -297,6 +297,9 @@ bool valid_common(int flux, int lim, int bc_x, int bc_y) {
 
 }  // namespace
 
+// Lets the library's other translation units report through fv_last_error().
+int fv_internal_set_error(int code, const char* msg) { return set_error(code, "%s", msg ? msg : ""); }
+
 extern "C" {
 
 const char* fv_last_error(void) { return g_last_error.c_str(); }

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(GridDesc g) {
 // After the state changed from outside the stage kernels: W = to_primitive(U), and the wave speeds /
 // positivity of U into slot step&1.
 constexpr int RED_NT = 256;
-__global__ void __launch_bounds__(RED_NT) wave_speed_kernel(const Q4* __restrict__ U, Q4* __restrict__ W, int n,
+static __global__ void __launch_bounds__(RED_NT) wave_speed_kernel(const Q4* __restrict__ U, Q4* __restrict__ W, int n,
                                                             FvCtrl* c) {
     const int par = int(c->step & 1);
     double sx = 0.0, sy = 0.0;
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(RED_NT) wave_speed_kernel(const Q4* __restrict
     reduce_wave_speeds<RED_NT>(sx, sy, bad, c, par);
 }
 
-__global__ void ctrl_reset_kernel(FvCtrl* c, double t, int reset_step) {
+static __global__ void ctrl_reset_kernel(FvCtrl* c, double t, int reset_step) {
     if (reset_step) c->step = 0;
     const int par = int(c->step & 1);
     c->sxy[par][0] = 0ull;
@@ -332,17 +332,17 @@ __global__ void ctrl_reset_kernel(FvCtrl* c, double t, int reset_step) {
     c->run2 = 0;
 }
 
-__global__ void ctrl_set_kernel(FvCtrl* c, int mode, double t_next, double dt_fixed) {
+static __global__ void ctrl_set_kernel(FvCtrl* c, int mode, double t_next, double dt_fixed) {
     c->mode = mode;
     c->t_next = t_next;
     c->dt_fixed = dt_fixed;
     if (mode == MODE_LOOP) c->status = 0;
 }
 
-__global__ void ctrl_set_time_kernel(FvCtrl* c, double t) { c->t[int(c->step & 1)] = t; }
+static __global__ void ctrl_set_time_kernel(FvCtrl* c, double t) { c->t[int(c->step & 1)] = t; }
 
 // to_conserved of primitive fields (io_hdf5.hpp:197-204); counts cells with !(rho>0)||!(p>0).
-__global__ void primitive_to_state_kernel(const double* __restrict__ rho, const double* __restrict__ u,
+static __global__ void primitive_to_state_kernel(const double* __restrict__ rho, const double* __restrict__ u,
                                           const double* __restrict__ v, const double* __restrict__ p, int n,
                                           Q4* __restrict__ U, int* nbad) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -354,7 +354,7 @@ __global__ void primitive_to_state_kernel(const double* __restrict__ rho, const 
 
 // TrajectoryWriter::add for one level (trajectory.hpp:31-51): one thread per coarse cell, the f x f
 // sum in j-outer / i-inner order, times inv = 1.0/(double(f)*f), cast to float.
-__global__ void block_average_kernel(const Q4* __restrict__ U, int nx, int ny, int f, double inv,
+static __global__ void block_average_kernel(const Q4* __restrict__ U, int nx, int ny, int f, double inv,
                                      float* __restrict__ out) {
     const int nxc = nx / f, nyc = ny / f;
     const int n = nxc * nyc;
@@ -387,7 +387,7 @@ __global__ void riemann_flux_kernel(int n, int y_face, const Q4* __restrict__ UL
 }
 
 // Ghosted copy of an interior state: cell (i, j) of the ring holds U[bc_index(i), bc_index(j)].
-__global__ void fill_ghosts_kernel(int nx, int ny, int bc_x, int bc_y, const Q4* __restrict__ U, Q4* __restrict__ Ug) {
+static __global__ void fill_ghosts_kernel(int nx, int ny, int bc_x, int bc_y, const Q4* __restrict__ U, Q4* __restrict__ Ug) {
     const int W = nx + 4, n = W * (ny + 4);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int j = k / W - 2, i = k % W - 2;
