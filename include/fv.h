@@ -111,6 +111,30 @@ int fv_block_average_device(fv_solver* s, int factor, float* d_out);
 int fv_run_trajectory(fv_solver* s, double t_start, double t_end, int nout, const int* sizes, int nsizes,
                       float** out, double* times, long long* steps, fv_bad_cell* bad);
 
+/* ---- Batched ensemble --------------------------------------------------------------------------
+ * Many independent grids ("members", uneven sizes allowed) with one flux and limiter, each keeping
+ * its own CFL dt, time and step count, advanced together: one persistent launch per RK stage covers
+ * the tiles of every running member, and batches of steps replay a captured CUDA graph.  Replaces
+ * running the driver once per trajectory (data/generate.py:60-105, solver_baseline.py:116-117).
+ * Every member is bit-identical to its own fv_advance_to run.
+ * bounds: 4*count doubles (x_min, x_max, y_min, y_max per member) or NULL for [0,1]^2. */
+typedef struct fv_ensemble fv_ensemble;
+int fv_ensemble_create(int count, const int* nx, const int* ny, const double* bounds, const int* bc_x,
+                       const int* bc_y, int flux, int limiter, double cfl, void* stream, fv_ensemble** out);
+int fv_ensemble_destroy(fv_ensemble* e);
+/* Member state in/out (interior layout above); setting resets the member's time and step count. */
+int fv_ensemble_set_state(fv_ensemble* e, int member, const double* U);
+int fv_ensemble_set_state_device(fv_ensemble* e, int member, const double* dU);
+int fv_ensemble_get_state(fv_ensemble* e, int member, double* U);
+/* Device address of a member's state (owned by the ensemble). */
+int fv_ensemble_state_device(fv_ensemble* e, int member, double** dU);
+/* Every member runs the driver loop (main2d.cpp:237-242) to its own t_next[member].  t, steps and
+ * status (each count entries, may be NULL) receive the members' times, step counts and statuses
+ * (0 or FV_ERR_NONPHYSICAL); a member that fails stops where compute_dt would have exited while the
+ * others continue, and the call then returns FV_ERR_NONPHYSICAL. */
+int fv_ensemble_advance_to(fv_ensemble* e, const double* t_next, double* t, long long* steps, int* status);
+int fv_ensemble_launch_count(fv_ensemble* e, long long* launches);
+
 /* Face fluxes of n face pairs evaluated on the GPU by the same device code the stage kernels use:
  * the FluxFn (riemann2d.hpp:8; rusanov_flux :11-15, hllc_flux :27-39) for y_face = 0, or
  * flux_y_face (riemann2d.hpp:42-44) for y_face = 1.  UL, UR, F: host arrays of n x 4 doubles.

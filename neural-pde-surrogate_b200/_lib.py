@@ -56,6 +56,14 @@ _PROTOS = {
     "fv_profile_read": [_P, _DP, _DP, _LLP],
     "fv_launch_count": [_P, _LLP],
     "fv_fp64_peak": [_DP],
+    "fv_ensemble_create": [_I, _P, _P, _P, _P, _P, _I, _I, _D, _P, C.POINTER(_P)],
+    "fv_ensemble_destroy": [_P],
+    "fv_ensemble_set_state": [_P, _I, _P],
+    "fv_ensemble_set_state_device": [_P, _I, _P],
+    "fv_ensemble_get_state": [_P, _I, _P],
+    "fv_ensemble_state_device": [_P, _I, C.POINTER(_P)],
+    "fv_ensemble_advance_to": [_P, _P, _P, _P, _P],
+    "fv_ensemble_launch_count": [_P, _LLP],
     "fv_autotune": [_P, _I, C.POINTER(_I)],
     "fv_set_tile": [_P, _I],
     "fv_get_tile": [_P, C.POINTER(_I)],

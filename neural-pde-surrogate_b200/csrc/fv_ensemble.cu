@@ -1,0 +1,378 @@
+// Batched ensemble: many independent grids (members) of uneven sizes, each with its own CFL dt, time
+// and step count, advanced together.  The reference runs one process per trajectory (data/generate.py:
+// 60-105, experiments/solver_baseline.py:116-117); here one persistent launch per RK stage covers the
+// tiles of every member still running, and batches of steps are replayed from a captured CUDA graph.
+//
+// Each member's arithmetic is the single-grid stage kernel's tile body with that member's own control
+// block (the CTA that handles a member's first tile is its leader), so every member is bit-identical
+// to its own fv_advance_to run.  Members that reached their target time skip their tiles.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/fv.h"
+#include "fv_kernels.cuh"
+
+int fv_internal_set_error(int code, const char* msg);
+
+using namespace fv;
+
+namespace {
+
+constexpr int TX = 16, TY = 16, NT = 256, MINB = 4;  // the shape the autotuner picks for 256^2-512^2
+using Smem = TileSmem<TX, TY>;
+
+struct Tile {
+    int member, i0, j0, leader;
+};
+
+// One RK stage for every tile of every running member.  Persistent: gridDim.x CTAs stride over the
+// tile table.
+template <int FLUX, int LIM, int STAGE>
+__global__ void __launch_bounds__(NT, MINB) ensemble_stage_kernel(const GridDesc* __restrict__ members,
+                                                                  const Tile* __restrict__ tiles, int ntiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& s = *reinterpret_cast<Smem*>(smem_raw);
+    __shared__ double s_dt;
+    __shared__ int s_go, s_par2;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const Tile tile = tiles[t];
+        const GridDesc g = members[tile.member];
+        FvCtrl* c = g.ctrl;
+        if (threadIdx.x == 0) {
+            double dt;
+            int go, par2 = 0;
+            if constexpr (STAGE == 1) {
+                go = stage1_control(c, g, tile.leader != 0, dt);
+            } else {
+                go = c->run2;
+                dt = c->dt;
+                par2 = c->par2;
+            }
+            s_go = go; s_dt = dt; s_par2 = par2;
+        }
+        __syncthreads();
+        if (s_go) {
+            double sx = 0.0, sy = 0.0;
+            int bad = INT_MAX;
+            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, tile.i0, tile.j0, s_dt, s, sx, sy, bad);
+            if constexpr (STAGE == 2) {
+                reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
+                if (tile.leader && threadIdx.x == 0) c->step = c->step + 1;
+            }
+        }
+        __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
+__global__ void ensemble_set_kernel(FvCtrl* ctrl, const double* t_next, int count) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= count) return;
+    ctrl[m].mode = MODE_LOOP;
+    ctrl[m].t_next = t_next[m];
+    ctrl[m].status = 0;
+}
+
+using StageFn = void (*)(const GridDesc*, const Tile*, int);
+
+template <int F, int L>
+void pick(StageFn* s1, StageFn* s2) {
+    *s1 = ensemble_stage_kernel<F, L, 1>;
+    *s2 = ensemble_stage_kernel<F, L, 2>;
+}
+
+void stage_pair(int flux, int lim, StageFn* s1, StageFn* s2) {
+    if (flux == FLUX_HLLC) {
+        if (lim == LIM_NONE) pick<FLUX_HLLC, LIM_NONE>(s1, s2);
+        else if (lim == LIM_UNLIMITED) pick<FLUX_HLLC, LIM_UNLIMITED>(s1, s2);
+        else if (lim == LIM_MINMOD) pick<FLUX_HLLC, LIM_MINMOD>(s1, s2);
+        else pick<FLUX_HLLC, LIM_VANLEER>(s1, s2);
+    } else {
+        if (lim == LIM_NONE) pick<FLUX_RUSANOV, LIM_NONE>(s1, s2);
+        else if (lim == LIM_UNLIMITED) pick<FLUX_RUSANOV, LIM_UNLIMITED>(s1, s2);
+        else if (lim == LIM_MINMOD) pick<FLUX_RUSANOV, LIM_MINMOD>(s1, s2);
+        else pick<FLUX_RUSANOV, LIM_VANLEER>(s1, s2);
+    }
+}
+
+}  // namespace
+
+struct fv_ensemble {
+    int count = 0, flux = 0, lim = 0;
+    double cfl = 0.5;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<GridDesc> h_members;   // host copy of the member descriptors
+    std::vector<size_t> offset;        // first cell of each member in the state pool
+    std::vector<int> has_state;
+    size_t total_cells = 0;
+    Q4* pool = nullptr;                // U | U1 | W | W1, each total_cells
+    FvCtrl* ctrl = nullptr;
+    FvCtrl* h_ctrl = nullptr;          // pinned mirror
+    GridDesc* d_members = nullptr;
+    Tile* d_tiles = nullptr;
+    int ntiles = 0;
+    double* d_tnext = nullptr;
+    double* h_tnext = nullptr;         // pinned staging
+    StageFn s1 = nullptr, s2 = nullptr;
+    int grid = 0;
+    cudaGraphExec_t graph = nullptr;   // kGraphSteps ensemble steps
+    static constexpr int kGraphSteps = 16;
+    long long launches = 0;
+};
+
+namespace {
+
+int err(int code, const char* msg) { return fv_internal_set_error(code, msg); }
+
+#define EN_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) return err(FV_ERR_CUDA, cudaGetErrorString(e_));        \
+    } while (0)
+
+int enqueue_steps(fv_ensemble* e, int nsteps) {
+    for (int k = 0; k < nsteps; ++k) {
+        e->s1<<<e->grid, NT, sizeof(Smem), e->stream>>>(e->d_members, e->d_tiles, e->ntiles);
+        e->s2<<<e->grid, NT, sizeof(Smem), e->stream>>>(e->d_members, e->d_tiles, e->ntiles);
+    }
+    EN_CUDA(cudaGetLastError());
+    return FV_OK;
+}
+
+int build_graph(fv_ensemble* e) {
+    cudaGraph_t g = nullptr;
+    EN_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_steps(e, fv_ensemble::kGraphSteps);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return err(FV_ERR_CUDA, cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return err(FV_ERR_CUDA, cudaGetErrorString(ce));
+    return FV_OK;
+}
+
+int read_ctrl(fv_ensemble* e) {
+    EN_CUDA(cudaMemcpyAsync(e->h_ctrl, e->ctrl, sizeof(FvCtrl) * e->count, cudaMemcpyDeviceToHost, e->stream));
+    EN_CUDA(cudaStreamSynchronize(e->stream));
+    return FV_OK;
+}
+
+int prime_member(fv_ensemble* e, int m) {
+    const GridDesc& g = e->h_members[m];
+    ctrl_reset_kernel<<<1, 1, 0, e->stream>>>(g.ctrl, 0.0, 1);
+    const int n = g.nx * g.ny;
+    wave_speed_kernel<<<std::max(1, std::min((n + RED_NT - 1) / RED_NT, 148 * 8)), RED_NT, 0, e->stream>>>(
+        g.U, g.W, n, g.ctrl);
+    e->launches += 2;
+    EN_CUDA(cudaGetLastError());
+    e->has_state[m] = 1;
+    return FV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fv_ensemble_create(int count, const int* nx, const int* ny, const double* bounds, const int* bc_x,
+                       const int* bc_y, int flux, int limiter, double cfl, void* stream, fv_ensemble** out) {
+    if (!out || count <= 0 || !nx || !ny || !bc_x || !bc_y) return err(FV_ERR_ARG, "fv_ensemble_create: bad arguments");
+    *out = nullptr;
+    if ((flux != FLUX_HLLC && flux != FLUX_RUSANOV) || limiter < LIM_NONE || limiter > LIM_VANLEER || !(cfl > 0.0))
+        return err(FV_ERR_ARG, "fv_ensemble_create: unknown flux/limiter or bad cfl");
+    size_t total = 0;
+    for (int m = 0; m < count; ++m) {
+        if (nx[m] <= 0 || ny[m] <= 0 || (long long)nx[m] * ny[m] > INT_MAX / 2)
+            return err(FV_ERR_ARG, "fv_ensemble_create: member grid sizes must be positive");
+        if ((bc_x[m] != BC_PERIODIC && bc_x[m] != BC_TRANSMISSIVE) || (bc_y[m] != BC_PERIODIC && bc_y[m] != BC_TRANSMISSIVE))
+            return err(FV_ERR_ARG, "fv_ensemble_create: unknown bc id");
+        if (bounds && (!(bounds[4 * m + 1] > bounds[4 * m]) || !(bounds[4 * m + 3] > bounds[4 * m + 2])))
+            return err(FV_ERR_ARG, "fv_ensemble_create: empty domain");
+        total += size_t(nx[m]) * ny[m];
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return err(FV_ERR_CUDA, "fv_ensemble_create: no CUDA device available");
+
+    fv_ensemble* e = new fv_ensemble;
+    e->count = count; e->flux = flux; e->lim = limiter; e->cfl = cfl;
+    e->total_cells = total;
+    stage_pair(flux, limiter, &e->s1, &e->s2);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e->grid = sms * MINB;
+    int rc = FV_OK;
+    auto fail = [&](cudaError_t ce) { if (rc == FV_OK) rc = err(FV_ERR_CUDA, cudaGetErrorString(ce)); };
+    cudaError_t ce;
+    if (stream) e->stream = (cudaStream_t)stream;
+    else if ((ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess) fail(ce);
+    else e->own_stream = true;
+    if (rc == FV_OK && (ce = cudaMalloc(&e->pool, 4 * total * sizeof(Q4))) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMalloc(&e->ctrl, count * sizeof(FvCtrl))) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMallocHost(&e->h_ctrl, count * sizeof(FvCtrl))) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMalloc(&e->d_members, count * sizeof(GridDesc))) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMalloc(&e->d_tnext, count * sizeof(double))) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMallocHost(&e->h_tnext, count * sizeof(double))) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMemsetAsync(e->ctrl, 0, count * sizeof(FvCtrl), e->stream)) != cudaSuccess) fail(ce);
+    std::vector<Tile> tiles;
+    if (rc == FV_OK) {
+        e->h_members.resize(count);
+        e->offset.resize(count);
+        e->has_state.assign(count, 0);
+        size_t off = 0;
+        for (int m = 0; m < count; ++m) {
+            GridDesc& g = e->h_members[m];
+            const double x0 = bounds ? bounds[4 * m] : 0.0, x1 = bounds ? bounds[4 * m + 1] : 1.0;
+            const double y0 = bounds ? bounds[4 * m + 2] : 0.0, y1 = bounds ? bounds[4 * m + 3] : 1.0;
+            g.nx = nx[m]; g.ny = ny[m]; g.bc_x = bc_x[m]; g.bc_y = bc_y[m];
+            g.dx = (x1 - x0) / nx[m];  // make_grid, grid2d.hpp:34-35
+            g.dy = (y1 - y0) / ny[m];
+            g.cfl = cfl;
+            g.cx = 1.0 / g.dx;
+            g.cy = 1.0 / g.dy;
+            e->offset[m] = off;
+            g.U = e->pool + off;
+            g.U1 = e->pool + total + off;
+            g.W = e->pool + 2 * total + off;
+            g.W1 = e->pool + 3 * total + off;
+            g.ctrl = e->ctrl + m;
+            off += size_t(nx[m]) * ny[m];
+        }
+        // tile table, largest members first (they run longest); a member's first tile leads it
+        std::vector<int> order(count);
+        for (int m = 0; m < count; ++m) order[m] = m;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return (long long)nx[a] * ny[a] > (long long)nx[b] * ny[b];
+        });
+        for (int m : order) {
+            bool first = true;
+            for (int j0 = 0; j0 < ny[m]; j0 += TY)
+                for (int i0 = 0; i0 < nx[m]; i0 += TX) {
+                    tiles.push_back(Tile{m, i0, j0, first ? 1 : 0});
+                    first = false;
+                }
+        }
+        e->ntiles = (int)tiles.size();
+        if ((ce = cudaMalloc(&e->d_tiles, tiles.size() * sizeof(Tile))) != cudaSuccess) fail(ce);
+    }
+    if (rc == FV_OK && (ce = cudaMemcpy(e->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice)) != cudaSuccess) fail(ce);
+    if (rc == FV_OK && (ce = cudaMemcpy(e->d_members, e->h_members.data(), count * sizeof(GridDesc), cudaMemcpyHostToDevice)) != cudaSuccess) fail(ce);
+    for (StageFn f : {e->s1, e->s2})
+        if (rc == FV_OK && (ce = cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem))) != cudaSuccess) fail(ce);
+    if (rc != FV_OK) {
+        fv_ensemble_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return FV_OK;
+}
+
+int fv_ensemble_destroy(fv_ensemble* e) {
+    if (!e) return FV_OK;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    cudaFree(e->pool);
+    cudaFree(e->ctrl);
+    cudaFree(e->d_members);
+    cudaFree(e->d_tiles);
+    cudaFree(e->d_tnext);
+    cudaFreeHost(e->h_ctrl);
+    cudaFreeHost(e->h_tnext);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return FV_OK;
+}
+
+int fv_ensemble_set_state(fv_ensemble* e, int m, const double* U) {
+    if (!e || !U || m < 0 || m >= e->count) return err(FV_ERR_ARG, "fv_ensemble_set_state: bad arguments");
+    const GridDesc& g = e->h_members[m];
+    EN_CUDA(cudaMemcpyAsync(g.U, U, size_t(g.nx) * g.ny * sizeof(Q4), cudaMemcpyHostToDevice, e->stream));
+    return prime_member(e, m);
+}
+
+int fv_ensemble_set_state_device(fv_ensemble* e, int m, const double* dU) {
+    if (!e || !dU || m < 0 || m >= e->count) return err(FV_ERR_ARG, "fv_ensemble_set_state_device: bad arguments");
+    const GridDesc& g = e->h_members[m];
+    EN_CUDA(cudaMemcpyAsync(g.U, dU, size_t(g.nx) * g.ny * sizeof(Q4), cudaMemcpyDeviceToDevice, e->stream));
+    return prime_member(e, m);
+}
+
+int fv_ensemble_get_state(fv_ensemble* e, int m, double* U) {
+    if (!e || !U || m < 0 || m >= e->count) return err(FV_ERR_ARG, "fv_ensemble_get_state: bad arguments");
+    const GridDesc& g = e->h_members[m];
+    EN_CUDA(cudaMemcpyAsync(U, g.U, size_t(g.nx) * g.ny * sizeof(Q4), cudaMemcpyDeviceToHost, e->stream));
+    EN_CUDA(cudaStreamSynchronize(e->stream));
+    return FV_OK;
+}
+
+int fv_ensemble_state_device(fv_ensemble* e, int m, double** dU) {
+    if (!e || !dU || m < 0 || m >= e->count) return err(FV_ERR_ARG, "fv_ensemble_state_device: bad arguments");
+    *dU = reinterpret_cast<double*>(e->h_members[m].U);
+    return FV_OK;
+}
+
+int fv_ensemble_advance_to(fv_ensemble* e, const double* t_next, double* t_out, long long* steps_out, int* status_out) {
+    if (!e || !t_next) return err(FV_ERR_ARG, "fv_ensemble_advance_to: bad arguments");
+    for (int m = 0; m < e->count; ++m)
+        if (!e->has_state[m]) return err(FV_ERR_STATE, "fv_ensemble_advance_to: a member has no state");
+    std::memcpy(e->h_tnext, t_next, e->count * sizeof(double));
+    EN_CUDA(cudaMemcpyAsync(e->d_tnext, e->h_tnext, e->count * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    ensemble_set_kernel<<<(e->count + 127) / 128, 128, 0, e->stream>>>(e->ctrl, e->d_tnext, e->count);
+    e->launches++;
+    EN_CUDA(cudaGetLastError());
+    if (!e->graph) {
+        int rc = build_graph(e);
+        if (rc) return rc;
+    }
+    int rc = read_ctrl(e);
+    if (rc) return rc;
+    for (;;) {
+        // steps still needed by the slowest member, from each member's current CFL dt
+        double need = 0.0;
+        for (int m = 0; m < e->count; ++m) {
+            const FvCtrl& c = e->h_ctrl[m];
+            const double t = c.t[c.step & 1];
+            if (c.status || !(t < t_next[m])) continue;
+            double sx, sy;
+            std::memcpy(&sx, &c.sxy[c.step & 1][0], 8);
+            std::memcpy(&sy, &c.sxy[c.step & 1][1], 8);
+            const GridDesc& g = e->h_members[m];
+            const double dt = e->cfl / (sx / g.dx + sy / g.dy);
+            need = std::max(need, dt > 0.0 ? std::ceil((t_next[m] - t) / dt) : 1.0);
+        }
+        if (need <= 0.0) break;
+        // whole graph replays (kGraphSteps steps each) while far from the end, single steps near it
+        int graphs = (int)std::min(need / fv_ensemble::kGraphSteps, 64.0);
+        for (int k = 0; k < graphs; ++k) EN_CUDA(cudaGraphLaunch(e->graph, e->stream));
+        e->launches += 2LL * fv_ensemble::kGraphSteps * graphs;
+        if (graphs == 0) {
+            const int few = (int)std::min(need, (double)fv_ensemble::kGraphSteps);
+            if ((rc = enqueue_steps(e, few))) return rc;
+            e->launches += 2LL * few;
+        }
+        if ((rc = read_ctrl(e))) return rc;
+    }
+    int worst = FV_OK;
+    for (int m = 0; m < e->count; ++m) {
+        const FvCtrl& c = e->h_ctrl[m];
+        if (t_out) t_out[m] = c.t[c.step & 1];
+        if (steps_out) steps_out[m] = c.step;
+        if (status_out) status_out[m] = c.status;
+        if (c.status) worst = c.status;
+    }
+    if (worst) return err(worst, "fv_ensemble_advance_to: a member reached a non-physical state (see status)");
+    return FV_OK;
+}
+
+int fv_ensemble_launch_count(fv_ensemble* e, long long* n) {
+    if (!e || !n) return err(FV_ERR_ARG, "fv_ensemble_launch_count: bad arguments");
+    *n = e->launches;
+    return FV_OK;
+}
+
+}  // extern "C"
