@@ -126,6 +126,10 @@ int fv_ensemble_destroy(fv_ensemble* e);
 int fv_ensemble_set_state(fv_ensemble* e, int member, const double* U);
 int fv_ensemble_set_state_device(fv_ensemble* e, int member, const double* dU);
 int fv_ensemble_get_state(fv_ensemble* e, int member, double* U);
+/* All members' states at once, from/to one device buffer holding them back to back in member order
+ * (sum of nx*ny*4 doubles); setting resets every member's time and step count. */
+int fv_ensemble_set_all_device(fv_ensemble* e, const double* dU);
+int fv_ensemble_get_all_device(fv_ensemble* e, double* dU);
 /* Device address of a member's state (owned by the ensemble). */
 int fv_ensemble_state_device(fv_ensemble* e, int member, double** dU);
 /* Every member runs the driver loop (main2d.cpp:237-242) to its own t_next[member].  t, steps and

@@ -64,6 +64,19 @@ _PROTOS = {
     "fv_ensemble_state_device": [_P, _I, C.POINTER(_P)],
     "fv_ensemble_advance_to": [_P, _P, _P, _P, _P],
     "fv_ensemble_launch_count": [_P, _LLP],
+    "fv_ensemble_set_all_device": [_P, _P],
+    "fv_ensemble_get_all_device": [_P, _P],
+    # correction network (include/fvnet.h)
+    "fvnet_conv3x3": [_I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "fvnet_conv3x3_wgrad": [_I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],
+    "fvnet_wgrad_parts": [_I, _I],
+    "fvnet_pack_weights": [_I, _I, _I, _I, _P, _P, _P, _P],
+    "fvnet_prep_input": [_P, C.c_longlong, _P, _P, _P],
+    "fvnet_apply_correction": [_P, _P, _I, _I, _P, _P, _P, _P, _I, _P],
+    "fvnet_loss_grad": [_P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P],
+    "fvnet_adamw": [_P, _P, _P, _P, C.c_longlong, _P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                    C.c_float, _I, _P, _P],
+    "fvnet_norm_partials": [],
     "fv_autotune": [_P, _I, C.POINTER(_I)],
     "fv_set_tile": [_P, _I],
     "fv_get_tile": [_P, C.POINTER(_I)],

@@ -310,6 +310,24 @@ int fv_ensemble_get_state(fv_ensemble* e, int m, double* U) {
     return FV_OK;
 }
 
+// All members at once from/to one device buffer holding the members' states back to back in member
+// order (the ensemble's own pool has exactly that layout).
+int fv_ensemble_set_all_device(fv_ensemble* e, const double* dU) {
+    if (!e || !dU) return err(FV_ERR_ARG, "fv_ensemble_set_all_device: bad arguments");
+    EN_CUDA(cudaMemcpyAsync(e->pool, dU, e->total_cells * sizeof(Q4), cudaMemcpyDeviceToDevice, e->stream));
+    for (int m = 0; m < e->count; ++m) {
+        int rc = prime_member(e, m);
+        if (rc) return rc;
+    }
+    return FV_OK;
+}
+
+int fv_ensemble_get_all_device(fv_ensemble* e, double* dU) {
+    if (!e || !dU) return err(FV_ERR_ARG, "fv_ensemble_get_all_device: bad arguments");
+    EN_CUDA(cudaMemcpyAsync(dU, e->pool, e->total_cells * sizeof(Q4), cudaMemcpyDeviceToDevice, e->stream));
+    return FV_OK;
+}
+
 int fv_ensemble_state_device(fv_ensemble* e, int m, double** dU) {
     if (!e || !dU || m < 0 || m >= e->count) return err(FV_ERR_ARG, "fv_ensemble_state_device: bad arguments");
     *dU = reinterpret_cast<double*>(e->h_members[m].U);

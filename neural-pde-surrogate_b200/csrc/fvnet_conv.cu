@@ -1,0 +1,481 @@
+// Periodic 3x3 convolutions of the correction network on the sm_100a tensor cores (tcgen05.mma,
+// BF16 operands, FP32 accumulators in TMEM), forward and backward.
+//
+// Semantics follow the reference's PeriodicConv (surrogate/models.py:16-29): wrap-pad by 1, then a
+// VALID 3x3 cross-correlation with weight (c_out, c_in, 3, 3) and a bias; the hidden activation is
+// jax.nn.gelu's default tanh approximation (models.py:43-44).
+//
+// Layout: activations NHWC bf16 with the channel count padded to 16 or 32; weights packed for the
+// MMA B operand as [shift = ky*3+kx][c_in/8][c_out][8] (K-major core matrices, 16 bytes per row).
+//
+// Forward (implicit GEMM, M = pixels, N = c_out, K = 9 * c_in): a CTA owns 256 output pixels
+// (256/W image rows).  It stages the (rows + 2) input rows three times, shifted in x by kx - 1 with
+// periodic wrap, in the K-major layout [kx][c_in/8][pixel][8]; then for every shift (ky, kx) the A
+// operand of the 128-pixel M-tile is that copy started ky rows further -- a plain descriptor offset,
+// no im2col buffer.  Two M-tiles x 9 shifts x (c_in/16) K-steps of tcgen05.mma (M=128, K=16) go to
+// TMEM; the epilogue (tcgen05.ld, one accumulator row per thread) adds the bias and applies GELU, or
+// for the backward-data pass multiplies by GELU'(pre-activation of the layer below).
+// Backward data is the same kernel with the weights transposed (c_in <-> c_out) and flipped.
+// Backward weights (M = 9 * c_in, N = c_out, K = pixels): per image row, the shifted input rows and
+// the output gradient are transposed into K-major tiles and accumulated in TMEM over the CTA's rows;
+// per-CTA partial sums are reduced in a fixed order (deterministic).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "../../include/fvnet.h"
+#include "tc_sm100.cuh"
+
+int fv_internal_set_error(int code, const char* msg);
+
+namespace fvnet {
+
+constexpr int NT = 128;
+constexpr float kGeluC0 = 0.7978845608028654f;  // sqrt(2/pi)
+constexpr float kGeluC1 = 0.044715f;
+
+__device__ __forceinline__ float gelu_tanh(float z) {
+    const float t = tanhf(kGeluC0 * (z + kGeluC1 * z * z * z));
+    return 0.5f * z * (1.0f + t);
+}
+__device__ __forceinline__ float gelu_tanh_grad(float z) {
+    const float t = tanhf(kGeluC0 * (z + kGeluC1 * z * z * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC0 * (1.0f + 3.0f * kGeluC1 * z * z);
+}
+
+struct ConvArgs {
+    const uint4* X;       // [B][H][W][CIN] bf16, as 16-byte chunks
+    const uint4* Wb;      // packed weights [9][CIN/8][COUT][8] bf16
+    const float* bias;    // [COUT] (forward modes)
+    const __nv_bfloat16* Zprev;  // [B][H][W][COUT] (mode BWD_GELU)
+    __nv_bfloat16* Z;     // [B][H][W][COUT] pre-activation (mode HIDDEN)
+    __nv_bfloat16* A;     // [B][H][W][COUT] activation (HIDDEN) or input gradient (BWD_*)
+    float* out4;          // [B][H][W][4] (mode OUTPUT)
+    int B, H, W;
+    int* err;
+};
+
+__device__ __forceinline__ uint4 pack8(const float* v) {
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(v[0], v[1]), p1 = __floats2bfloat162_rn(v[2], v[3]);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(v[4], v[5]), p3 = __floats2bfloat162_rn(v[6], v[7]);
+    uint4 u;
+    u.x = *reinterpret_cast<uint32_t*>(&p0);
+    u.y = *reinterpret_cast<uint32_t*>(&p1);
+    u.z = *reinterpret_cast<uint32_t*>(&p2);
+    u.w = *reinterpret_cast<uint32_t*>(&p3);
+    return u;
+}
+
+__host__ __device__ constexpr size_t conv_smem_bytes(int cin, int cout, int W) {
+    return size_t(3) * (cin / 8) * ((256 / W + 2) * W) * 16 + size_t(9) * (cin / 8) * cout * 16 + 64;
+}
+
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(NT) conv3x3_kernel(ConvArgs a) {
+    constexpr int CC = CIN / 8;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int W = a.W, H = a.H;
+    const int TR = 256 / W, NPIX = (TR + 2) * W;
+    uint4* Xc = reinterpret_cast<uint4*>(smem);                  // [3][CC][NPIX]
+    uint4* Wt = Xc + size_t(3) * CC * NPIX;                      // [9][CC][COUT]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Wt + 9 * CC * COUT);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n = blockIdx.y, y0 = blockIdx.x * TR;
+    constexpr uint32_t kCols = (2 * COUT) < 32 ? 32 : 2 * COUT;
+
+    if (warp == 0) tc::tmem_alloc(tslot, kCols);
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    // stage three x-shifted copies of rows y0-1 .. y0+TR (periodic in x and y)
+    for (int e = tid; e < (TR + 2) * W * CC; e += NT) {
+        const int cc = e % CC, t = e / CC, x = t % W, r = t / W;
+        const int y = (y0 - 1 + r + H) % H;
+        const uint4 v = a.X[(size_t(n * H + y) * W + x) * CC + cc];
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) {
+            const int xd = (x - kx + 1 + W) % W;
+            Xc[(size_t(kx) * CC + cc) * NPIX + r * W + xd] = v;
+        }
+    }
+    for (int e = tid; e < 9 * CC * COUT; e += NT) Wt[e] = a.Wb[e];
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (tid == 0) {
+        constexpr uint32_t idesc = tc::idesc_bf16_f32(128, COUT);
+        const uint32_t xb = tc::smem_addr(Xc), wb = tc::smem_addr(Wt);
+        const uint32_t lbo_a = uint32_t(NPIX) * 16, lbo_b = COUT * 16;
+        for (int mt = 0; mt < 2; ++mt)
+            for (int sh = 0; sh < 9; ++sh) {
+                const int ky = sh / 3, kx = sh % 3;
+                for (int s = 0; s < CIN / 16; ++s) {
+                    const uint32_t aa = xb + ((kx * CC + 2 * s) * NPIX + mt * 128 + ky * W) * 16;
+                    const uint32_t ba = wb + (sh * CC + 2 * s) * COUT * 16;
+                    tc::mma_bf16(tmem + mt * COUT, tc::smem_desc(aa, lbo_a, 128), tc::smem_desc(ba, lbo_b, 128), idesc,
+                                 (sh | s) != 0);
+                }
+            }
+        tc::mma_commit(bar);
+    }
+    const bool ok = tc::mbar_wait_bounded(bar, 0, a.err);
+    tc::fence_after_sync();
+    if (ok) {
+        for (int mt = 0; mt < 2; ++mt) {
+            float acc[32];
+            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + mt * COUT;
+            if constexpr (COUT == 32) tc::tmem_ld_32x32(taddr, acc);
+            else tc::tmem_ld_32x16(taddr, acc);
+            const int m = mt * 128 + warp * 32 + lane;
+            const int r = m / W, x = m % W;
+            const size_t gp = size_t(n * H + y0 + r) * W + x;
+            if constexpr (MODE == FVNET_CONV_HIDDEN) {
+                float z[COUT], g[COUT];
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) {
+                    z[c] = acc[c] + a.bias[c];
+                    g[c] = gelu_tanh(z[c]);
+                }
+                uint4* Zo = reinterpret_cast<uint4*>(a.Z + gp * COUT);
+                uint4* Ao = reinterpret_cast<uint4*>(a.A + gp * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) {
+                    Zo[q] = pack8(z + 8 * q);
+                    Ao[q] = pack8(g + 8 * q);
+                }
+            } else if constexpr (MODE == FVNET_CONV_OUTPUT) {
+                float4 o = make_float4(acc[0] + a.bias[0], acc[1] + a.bias[1], acc[2] + a.bias[2], acc[3] + a.bias[3]);
+                reinterpret_cast<float4*>(a.out4)[gp] = o;
+            } else {
+                float d[COUT];
+                const uint4* Zp = reinterpret_cast<const uint4*>(a.Zprev + gp * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) {
+                    const uint4 u = Zp[q];
+                    const __nv_bfloat16* zb = reinterpret_cast<const __nv_bfloat16*>(&u);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float gz = (MODE == FVNET_CONV_BWD_GELU) ? gelu_tanh_grad(__bfloat162float(zb[j])) : 1.0f;
+                        d[8 * q + j] = acc[8 * q + j] * gz;
+                    }
+                }
+                uint4* Ao = reinterpret_cast<uint4*>(a.A + gp * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) Ao[q] = pack8(d + 8 * q);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+}
+
+// ---- backward weights --------------------------------------------------------------------------
+struct WgradArgs {
+    const uint4* X;   // [B][H][W][CIN]
+    const uint4* dZ;  // [B][H][W][COUT]
+    float* partial;   // [gridDim.x][9*CIN][COUT]
+    int B, H, W;
+    int rows_per_cta;
+    int* err;
+};
+
+__host__ __device__ constexpr int wgrad_mrows(int cin) { return ((9 * cin + 127) / 128) * 128; }
+__host__ __device__ constexpr size_t wgrad_smem_bytes(int cin, int cout, int W) {
+    return size_t(W / 8) * wgrad_mrows(cin) * 16 + size_t(W / 8) * cout * 16 + size_t(3) * W * cin * 2 +
+           size_t(W) * cout * 2 + 64;
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
+    constexpr int M9 = 9 * CIN, MROWS = wgrad_mrows(CIN), MT = MROWS / 128, CC = CIN / 8, OC = COUT / 8;
+    constexpr uint32_t kCols = (MT * COUT) <= 32 ? 32 : ((MT * COUT) <= 64 ? 64 : 128);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int W = a.W, H = a.H, KC = W / 8;
+    uint4* As = reinterpret_cast<uint4*>(smem);                 // [KC][MROWS]
+    uint4* Bs = As + size_t(KC) * MROWS;                        // [KC][COUT]
+    __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(Bs + KC * COUT);  // [3][W][CIN]
+    __nv_bfloat16* Ds = Xs + 3 * W * CIN;                        // [W][COUT]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + W * COUT);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int total = a.B * H;
+    const int r0 = blockIdx.x * a.rows_per_cta, r1 = min(total, r0 + a.rows_per_cta);
+
+    if (warp == 0) tc::tmem_alloc(tslot, kCols);
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    for (int e = tid; e < KC * MROWS; e += NT) As[e] = make_uint4(0, 0, 0, 0);  // padding rows stay zero
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, COUT);
+    const uint32_t ab = tc::smem_addr(As), bb = tc::smem_addr(Bs);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int row = r0; row < r1 && ok; ++row) {
+        const int n = row / H, y = row % H;
+        uint4* Xs4 = reinterpret_cast<uint4*>(Xs);
+        for (int e = tid; e < 3 * W * CC; e += NT) {
+            const int cc = e % CC, t = e / CC, x = t % W, ky = t / W;
+            const int yy = (y + ky - 1 + H) % H;
+            Xs4[e] = a.X[(size_t(n * H + yy) * W + x) * CC + cc];
+        }
+        uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
+        for (int e = tid; e < W * OC; e += NT) Ds4[e] = a.dZ[size_t(n * H + y) * W * OC + e];
+        __syncthreads();
+        // A[kc][m = shift*CIN + ci] = X[y+ky-1][kc*8 + i + kx - 1][ci], i = 0..7 (periodic)
+        for (int e = tid; e < KC * M9; e += NT) {
+            const int m = e % M9, kc = e / M9;
+            const int sh = m / CIN, ci = m % CIN, ky = sh / 3, kx = sh % 3;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int x = (kc * 8 + i + kx - 1 + W) % W;
+                v[i] = __bfloat162float(Xs[(ky * W + x) * CIN + ci]);
+            }
+            As[size_t(kc) * MROWS + m] = pack8(v);
+        }
+        // B[kc][co] = dZ[kc*8 + i][co]
+        for (int e = tid; e < KC * COUT; e += NT) {
+            const int co = e % COUT, kc = e / COUT;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = __bfloat162float(Ds[(kc * 8 + i) * COUT + co]);
+            Bs[e] = pack8(v);
+        }
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) {
+            for (int mt = 0; mt < MT; ++mt)
+                for (int ks = 0; ks < KC / 2; ++ks) {
+                    const uint32_t aa = ab + (2 * ks * MROWS + mt * 128) * 16;
+                    const uint32_t ba = bb + (2 * ks * COUT) * 16;
+                    tc::mma_bf16(tmem + mt * COUT, tc::smem_desc(aa, MROWS * 16, 128), tc::smem_desc(ba, COUT * 16, 128),
+                                 idesc, (row > r0 || ks > 0) ? 1u : 0u);
+                }
+            tc::mma_commit(bar);
+        }
+        ok = tc::mbar_wait_bounded(bar, phase, a.err);
+        phase ^= 1;
+        tc::fence_after_sync();
+    }
+    if (ok && r0 < r1) {
+        for (int mt = 0; mt < MT; ++mt) {
+            float acc[32];
+            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + mt * COUT;
+            if constexpr (COUT == 32) tc::tmem_ld_32x32(taddr, acc);
+            else tc::tmem_ld_32x16(taddr, acc);
+            const int m = mt * 128 + warp * 32 + lane;
+            if (m < M9) {
+                float* dst = a.partial + (size_t(blockIdx.x) * M9 + m) * COUT;
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) dst[c] = acc[c];
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+}
+
+// dW[co][ci][ky][kx] = sum over CTAs (fixed order) of partial[cta][(ky*3+kx)*cin_pad + ci][co]
+__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int nparts, int cin_pad, int cout_pad,
+                                    int cin, int cout, float* __restrict__ dW) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= cout * cin * 9) return;
+    const int k = e % 9, ci = (e / 9) % cin, co = e / (9 * cin);
+    const size_t stride = size_t(9) * cin_pad * cout_pad;
+    const size_t off = (size_t(k) * cin_pad + ci) * cout_pad + co;
+    float s = 0.0f;
+    for (int p = 0; p < nparts; ++p) s += partial[p * stride + off];
+    dW[e] = s;
+}
+
+// db[co] = sum over pixels of dZ[p][co]: block partials, then a fixed-order sum.
+__global__ void bias_grad_partial_kernel(const __nv_bfloat16* __restrict__ dZ, long long npix, int cout_pad, int cout,
+                                         float* __restrict__ part) {
+    __shared__ float s[NT];
+    for (int co = 0; co < cout; ++co) {
+        float acc = 0.0f;
+        for (long long p = blockIdx.x * (long long)NT + threadIdx.x; p < npix; p += (long long)gridDim.x * NT)
+            acc += __bfloat162float(dZ[p * cout_pad + co]);
+        s[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = NT / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[blockIdx.x * cout + co] = s[0];
+        __syncthreads();
+    }
+}
+__global__ void bias_grad_reduce_kernel(const float* __restrict__ part, int nparts, int cout, float* __restrict__ db) {
+    const int co = threadIdx.x;
+    if (co >= cout) return;
+    float s = 0.0f;
+    for (int p = 0; p < nparts; ++p) s += part[p * cout + co];
+    db[co] = s;
+}
+
+// Canonical fp32 weights W[co][ci][3][3] -> bf16 B-operand packs for the forward pass
+// ([sh][cin_pad/8][cout_pad][8]) and the backward-data pass (transposed, spatially flipped:
+// [sh'][cout_pad/8][cin_pad][8] with element W[co][ci][2-ky'][2-kx']).  Padding is zero.
+__global__ void pack_weights_kernel(const float* __restrict__ Wc, int cout, int cin, int cout_pad, int cin_pad,
+                                    __nv_bfloat16* __restrict__ Wf, __nv_bfloat16* __restrict__ Wbk) {
+    const int nf = 9 * cin_pad * cout_pad;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nf; e += gridDim.x * blockDim.x) {
+        // forward: e = ((sh*CC + cc)*cout_pad + co)*8 + j, ci = cc*8 + j
+        {
+            const int j = e % 8, co = (e / 8) % cout_pad, cc = (e / (8 * cout_pad)) % (cin_pad / 8),
+                      sh = e / (8 * cout_pad * (cin_pad / 8));
+            const int ci = cc * 8 + j, ky = sh / 3, kx = sh % 3;
+            const float w = (co < cout && ci < cin) ? Wc[((co * cin + ci) * 3 + ky) * 3 + kx] : 0.0f;
+            Wf[e] = __float2bfloat16_rn(w);
+        }
+        // backward data: e = ((sh*CC' + cc)*cin_pad + ci)*8 + j, co = cc*8 + j, CC' = cout_pad/8
+        {
+            const int j = e % 8, ci = (e / 8) % cin_pad, cc = (e / (8 * cin_pad)) % (cout_pad / 8),
+                      sh = e / (8 * cin_pad * (cout_pad / 8));
+            const int co = cc * 8 + j, ky = 2 - sh / 3, kx = 2 - sh % 3;
+            const float w = (co < cout && ci < cin) ? Wc[((co * cin + ci) * 3 + ky) * 3 + kx] : 0.0f;
+            Wbk[e] = __float2bfloat16_rn(w);
+        }
+    }
+}
+
+template <int CIN, int COUT, int MODE>
+int launch_conv(const ConvArgs& a, cudaStream_t st) {
+    const size_t smem = conv_smem_bytes(CIN, COUT, a.W);
+    static bool attr = false;
+    if (!attr) {  // the limit for the largest image width served (W = 256)
+        if (cudaFuncSetAttribute(conv3x3_kernel<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)conv_smem_bytes(CIN, COUT, 256)) != cudaSuccess)
+            return fv_internal_set_error(FVNET_ERR_CUDA, "fvnet: smem attribute");
+        attr = true;
+    }
+    dim3 grid(a.H / (256 / a.W), a.B);
+    conv3x3_kernel<CIN, COUT, MODE><<<grid, NT, smem, st>>>(a);
+    return FVNET_OK;
+}
+
+template <int CIN, int COUT>
+int launch_wgrad(const WgradArgs& a, int nparts, cudaStream_t st) {
+    const size_t smem = wgrad_smem_bytes(CIN, COUT, a.W);
+    static bool attr = false;
+    if (!attr) {  // the limit for the largest image width served (W = 128)
+        if (cudaFuncSetAttribute(conv3x3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)wgrad_smem_bytes(CIN, COUT, 128)) != cudaSuccess)
+            return fv_internal_set_error(FVNET_ERR_CUDA, "fvnet: smem attribute");
+        attr = true;
+    }
+    conv3x3_wgrad_kernel<CIN, COUT><<<nparts, NT, smem, st>>>(a);
+    return FVNET_OK;
+}
+
+bool shape_ok(int B, int H, int W) {
+    return B > 0 && (W == 32 || W == 64 || W == 128 || W == 256) && H > 0 && H % (256 / W) == 0;
+}
+
+}  // namespace fvnet
+
+using namespace fvnet;
+
+extern "C" {
+
+int fvnet_conv3x3(int mode, int cin_pad, int cout_pad, int B, int H, int W, const void* X, const void* Wpacked,
+                  const float* bias, const void* Zprev, void* Z, void* A, float* out4, int* err, void* stream) {
+    if (!shape_ok(B, H, W) || !X || !Wpacked) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3: bad shape or NULL input");
+    ConvArgs a{};
+    a.X = static_cast<const uint4*>(X);
+    a.Wb = static_cast<const uint4*>(Wpacked);
+    a.bias = bias;
+    a.Zprev = static_cast<const __nv_bfloat16*>(Zprev);
+    a.Z = static_cast<__nv_bfloat16*>(Z);
+    a.A = static_cast<__nv_bfloat16*>(A);
+    a.out4 = out4;
+    a.B = B; a.H = H; a.W = W; a.err = err;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = FVNET_ERR_ARG;
+    if (mode == FVNET_CONV_HIDDEN) {
+        if (!bias || !Z || !A) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3: hidden needs bias, Z, A");
+        if (cin_pad == 16 && cout_pad == 32) rc = launch_conv<16, 32, FVNET_CONV_HIDDEN>(a, st);
+        else if (cin_pad == 32 && cout_pad == 32) rc = launch_conv<32, 32, FVNET_CONV_HIDDEN>(a, st);
+    } else if (mode == FVNET_CONV_OUTPUT) {
+        if (!bias || !out4) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3: output needs bias, out4");
+        if (cin_pad == 32 && cout_pad == 16) rc = launch_conv<32, 16, FVNET_CONV_OUTPUT>(a, st);
+    } else if (mode == FVNET_CONV_BWD_GELU) {
+        if (!Zprev || !A) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3: backward needs Zprev, A");
+        if (cin_pad == 16 && cout_pad == 32) rc = launch_conv<16, 32, FVNET_CONV_BWD_GELU>(a, st);
+        else if (cin_pad == 32 && cout_pad == 32) rc = launch_conv<32, 32, FVNET_CONV_BWD_GELU>(a, st);
+    } else if (mode == FVNET_CONV_BWD_PLAIN) {
+        if (!A) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3: backward needs A");
+        if (cin_pad == 16 && cout_pad == 32) rc = launch_conv<16, 32, FVNET_CONV_BWD_PLAIN>(a, st);
+        else if (cin_pad == 32 && cout_pad == 32) rc = launch_conv<32, 32, FVNET_CONV_BWD_PLAIN>(a, st);
+        else if (cin_pad == 32 && cout_pad == 16) rc = launch_conv<32, 16, FVNET_CONV_BWD_PLAIN>(a, st);
+    }
+    if (rc == FVNET_ERR_ARG) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3: unsupported mode/channels");
+    if (rc) return rc;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fv_internal_set_error(FVNET_ERR_CUDA, cudaGetErrorString(e));
+    return FVNET_OK;
+}
+
+int fvnet_wgrad_parts(int B, int H) { return std::max(1, std::min(148, B * H)); }
+
+int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int H, int W, const void* X, const void* dZ,
+                        float* partial, float* dW, float* db, float* db_part, int* err, void* stream) {
+    if (!shape_ok(B, H, W) || W > 128 || !X || !dZ || !partial || !dW || !db || !db_part || cin > cin_pad ||
+        cout > cout_pad)
+        return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3_wgrad: bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nparts = fvnet_wgrad_parts(B, H);
+    WgradArgs a{};
+    a.X = static_cast<const uint4*>(X);
+    a.dZ = static_cast<const uint4*>(dZ);
+    a.partial = partial;
+    a.B = B; a.H = H; a.W = W;
+    a.rows_per_cta = (B * H + nparts - 1) / nparts;
+    a.err = err;
+    int rc = FVNET_ERR_ARG;
+    if (cin_pad == 16 && cout_pad == 32) rc = launch_wgrad<16, 32>(a, nparts, st);
+    else if (cin_pad == 32 && cout_pad == 32) rc = launch_wgrad<32, 32>(a, nparts, st);
+    else if (cin_pad == 32 && cout_pad == 16) rc = launch_wgrad<32, 16>(a, nparts, st);
+    if (rc == FVNET_ERR_ARG) return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_conv3x3_wgrad: unsupported channels");
+    if (rc) return rc;
+    // parts actually used: CTAs whose row range is not empty
+    const int used = (B * H + a.rows_per_cta - 1) / a.rows_per_cta;
+    wgrad_reduce_kernel<<<(cout * cin * 9 + 255) / 256, 256, 0, st>>>(partial, used, cin_pad, cout_pad, cin, cout, dW);
+    bias_grad_partial_kernel<<<64, NT, 0, st>>>(static_cast<const __nv_bfloat16*>(dZ), (long long)B * H * W, cout_pad,
+                                                cout, db_part);
+    bias_grad_reduce_kernel<<<1, 64, 0, st>>>(db_part, 64, cout, db);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fv_internal_set_error(FVNET_ERR_CUDA, cudaGetErrorString(e));
+    return FVNET_OK;
+}
+
+int fvnet_pack_weights(int cout, int cin, int cout_pad, int cin_pad, const float* W, void* Wfwd, void* Wbwd,
+                       void* stream) {
+    if (!W || !Wfwd || !Wbwd || cout > cout_pad || cin > cin_pad || cin_pad % 8 || cout_pad % 8)
+        return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_pack_weights: bad arguments");
+    const int nf = 9 * cin_pad * cout_pad;
+    pack_weights_kernel<<<(nf + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        W, cout, cin, cout_pad, cin_pad, static_cast<__nv_bfloat16*>(Wfwd), static_cast<__nv_bfloat16*>(Wbwd));
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fv_internal_set_error(FVNET_ERR_CUDA, cudaGetErrorString(e));
+    return FVNET_OK;
+}
+
+}  // extern "C"

@@ -54,6 +54,20 @@ class Ensemble:
             raise ValueError(f"member {k}: state must have shape {(g.ny, g.nx, 4)}")
         check(lib().fv_ensemble_set_state(self._h, int(k), C.c_void_p(U.ctypes.data)))
 
+    def set_all(self, U):
+        """All members from one CUDA float64 tensor holding their states back to back in member order
+        (e.g. shape (count, ny, nx, 4) when all members have one size)."""
+        assert getattr(U, "is_cuda", False) and U.is_contiguous() and str(U.dtype) == "torch.float64"
+        assert U.numel() == 4 * sum(g.nx * g.ny for g in self.grids)
+        check(lib().fv_ensemble_set_all_device(self._h, C.c_void_p(U.data_ptr())))
+
+    def get_all(self, out):
+        """All members' states into a CUDA float64 tensor (layout of set_all)."""
+        assert getattr(out, "is_cuda", False) and out.is_contiguous() and str(out.dtype) == "torch.float64"
+        assert out.numel() == 4 * sum(g.nx * g.ny for g in self.grids)
+        check(lib().fv_ensemble_get_all_device(self._h, C.c_void_p(out.data_ptr())))
+        return out
+
     def get_state(self, k):
         g = self.grids[k]
         out = np.empty((g.ny, g.nx, 4), np.float64)

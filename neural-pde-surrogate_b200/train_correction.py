@@ -1,0 +1,234 @@
+"""Train the coarse-grid correction on solver-generated data (the learned part, on the GPU).
+
+  python neural-pde-surrogate_b200/train_correction.py --out runs/corr --n-traj 512 --fine 512 \
+         --coarse 64 --steps 20000 --batch 64 --unroll 4 --lr 1e-3
+
+Data: n_traj trajectories (half four-quadrant Riemann, half blast + bubble initial conditions,
+indices [index0, index0 + n_traj/2) of each family) solved by the FP64 GPU solver at fine^2 and
+block-averaged to coarse^2 every 0.005 in time (generate.trajectory).  Normalisation statistics are
+taken from these training frames only (data/pack.py:54-112 does the same).
+
+Model step (correction.hybrid_step): the coarse FP64 solver advances one frame interval, the CNN
+adds a zero-mean (conservative) correction.  Loss: pushforward with `unroll` steps
+(surrogate/train.py:107-111): unroll-1 hybrid steps without gradient, then one trained step to the
+true frame t+unroll, MSE in normalised units.  Optimiser: clip by global norm 1.0 + AdamW (weight
+decay 1e-4) with warm-up + cosine decay to 0.01*lr (train.py:207-211).  Writes log.csv, config.json,
+best.npz / last.npz (parameters) like the reference's run folder (train.py:197-255).
+"""
+import argparse
+import csv
+import importlib
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+
+PKG = "neural-pde-surrogate_b200"
+DT_FRAME = 0.005
+
+
+def build_dataset(n_traj, fine, coarse, index0=0, families=("riemann", "blast"), frames=None, log=print):
+    """(N, F, coarse, coarse, 4) float64 CUDA tensor of block-averaged conserved states; F is the
+    shortest trajectory's frame count (every trajectory is truncated to it)."""
+    import torch
+    fv = importlib.import_module(PKG)
+    gen = importlib.import_module(f"{PKG}.generate")
+    solver = fv.Solver(fv.make_grid(fine, fine, 0.0, 1.0, 0.0, 1.0, "periodic", "periodic"), "hllc", "vanleer", 0.5)
+    out, t0, cells = [], time.time(), 0
+    per = max(1, n_traj // len(families))
+    for fam in families:
+        for k in range(per):
+            t, levels, steps, _ = gen.trajectory(fam, index0 + k, fine, [coarse], solver=solver)
+            out.append(levels[coarse])
+            cells += steps * fine * fine
+    nf = min(a.shape[0] for a in out) if frames is None else frames
+    data = np.stack([a[:nf] for a in out])  # (N, F, 4, c, c) float32
+    U = torch.from_numpy(np.ascontiguousarray(data.transpose(0, 1, 3, 4, 2))).to("cuda", torch.float64)
+    log(f"dataset: {len(out)} trajectories at {fine}^2 -> {coarse}^2, {nf} frames, {time.time() - t0:.1f} s "
+        f"({cells / max(time.time() - t0, 1e-9) / 1e9:.2f} G cell-updates/s incl. transfers)")
+    return U
+
+
+def field_stats(U):
+    """[mean(4), 1/std(4)] over every cell of every frame (FP64)."""
+    import torch
+    flat = U.reshape(-1, 4)
+    mean = flat.mean(dim=0)
+    std = flat.std(dim=0).clamp_min(1e-12)
+    return torch.cat([mean, 1.0 / std]).contiguous()
+
+
+def correction_weights(U):
+    """(rho, rho, rho, E) of each cell: the units of the network's corrections."""
+    import torch
+    return torch.stack([U[..., 0], U[..., 0], U[..., 0], U[..., 3]], dim=-1)
+
+
+def residual_scale(U, coarse_solver, B, rng, pairs=4):
+    """Per-field std of (next frame - coarse step of this frame) in the correction's units: the size of
+    what the network must add, so that its raw output is O(1) (the reference scales its output by
+    delta_std, models.py:65)."""
+    import torch
+    N, F = U.shape[:2]
+    acc = []
+    Uc = torch.empty((B,) + tuple(U.shape[2:]), dtype=torch.float64, device="cuda")
+    for _ in range(pairs):
+        i = torch.as_tensor(rng.integers(N, size=B), device="cuda")
+        t = torch.as_tensor(rng.integers(F - 1, size=B), device="cuda")
+        x = U[i, t].contiguous()
+        coarse_solver.advance(x, DT_FRAME, Uc)
+        acc.append(((U[i, t + 1] - Uc) / correction_weights(Uc)).reshape(-1, 4))
+    return torch.cat(acc).std(dim=0).clamp_min(1e-12).contiguous()
+
+
+class Trainer:
+    def __init__(self, train, val, batch, unroll, seed=0, log=print):
+        import torch
+        self.torch = torch
+        corr = importlib.import_module(f"{PKG}.correction")
+        self.corr = corr
+        self.train_U, self.val_U = train, val
+        self.B, self.unroll = batch, unroll
+        H, W = train.shape[2:4]
+        self.rng = np.random.default_rng(seed)
+        self.coarse = corr.CoarseSolver(batch, H, W)
+        self.net = corr.CorrectionNet(batch, H, W, seed=seed)
+        self.stats = field_stats(train)
+        self.dscale = residual_scale(train, self.coarse, batch, self.rng)
+        shape = (batch, H, W, 4)
+        self.x = torch.empty(shape, dtype=torch.float64, device="cuda")
+        self.Uc = torch.empty_like(self.x)
+        self.Un = torch.empty_like(self.x)
+        self.fb = torch.zeros(batch, dtype=torch.int32, device="cuda")
+        self.loss_part = torch.zeros(batch, dtype=torch.float64, device="cuda")
+        self.mode = "scale"  # positivity rule of the self-fed and evaluation steps
+        log(f"stats mean {self.stats[:4].tolist()} std {(1 / self.stats[4:]).tolist()}; "
+            f"residual scale {self.dscale.tolist()}")
+
+    def _pairs(self, U, k):
+        N, F = U.shape[:2]
+        i = self.torch.as_tensor(self.rng.integers(N, size=self.B), device="cuda")
+        t = self.torch.as_tensor(self.rng.integers(F - k, size=self.B), device="cuda")
+        return U[i, t].contiguous(), U[i, t + k].contiguous()
+
+    def step(self, lr, unroll=None):
+        """One pushforward training step; returns the loss tensor (not synchronised)."""
+        unroll = unroll or self.unroll
+        x, y = self._pairs(self.train_U, unroll)
+        self.x.copy_(x)
+        for _ in range(unroll - 1):  # self-fed steps, no gradient, physical by construction
+            self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un,
+                                  self.fb, mode=self.mode)
+            self.x.copy_(self.Un)
+        # the trained step keeps its full correction even where it is non-physical: the loss then pulls
+        # it toward the (physical) target instead of the sample dropping out of the gradient
+        self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un, self.fb,
+                              mode="keep")
+        self.net.loss_grad(self.Un, y, self.Uc, self.stats, self.dscale, None, self.loss_part)
+        self.net.backward()
+        self.net.adamw(lr)
+        return self.loss_part.sum() / (self.B * self.Un[0].numel())
+
+    def evaluate(self, U, batches=4, k=1, mode=None):
+        """Mean normalised MSE after k steps of (hybrid, coarse-only) on pairs drawn from U."""
+        h, c = 0.0, 0.0
+        inv = self.stats[4:]
+        self.fallback_count = 0
+        for _ in range(batches):
+            x, y = self._pairs(U, k)
+            xh = x.clone()
+            xc = x.clone()
+            for _ in range(k):
+                self.corr.hybrid_step(self.net, self.coarse, xh, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un,
+                                      self.fb, mode=mode or self.mode)
+                self.fallback_count += int(self.fb.sum())
+                xh.copy_(self.Un)
+                self.coarse.advance(xc, DT_FRAME, self.Uc)
+                xc.copy_(self.Uc)
+            h += float((((xh - y) * inv) ** 2).mean())
+            c += float((((xc - y) * inv) ** 2).mean())
+        return h / batches, c / batches
+
+
+def train(cfg, log=print):
+    """cfg: dict (see main()).  Returns (trainer, history rows)."""
+    import torch
+    out = Path(cfg["out"]) if cfg.get("out") else None
+    if out:
+        out.mkdir(parents=True, exist_ok=True)
+    t0 = time.time()
+    train_U = build_dataset(cfg["n_traj"], cfg["fine"], cfg["coarse"], index0=0, log=log)
+    val_U = build_dataset(cfg["n_val"], cfg["fine"], cfg["coarse"], index0=100000, log=log)
+    tr = Trainer(train_U, val_U, cfg["batch"], cfg["unroll"], seed=cfg["seed"], log=log)
+    corr = tr.corr
+    hist = []
+    writer = None
+    if out:
+        (out / "config.json").write_text(json.dumps({**cfg, "params": corr.param_count(),
+                                                      "stats": tr.stats.tolist(), "dscale": tr.dscale.tolist()},
+                                                     indent=2))
+        logf = open(out / "log.csv", "w", newline="")
+        writer = csv.writer(logf)
+        writer.writerow(["step", "train_loss", "val_hybrid", "val_coarse", "val_ratio", "lr", "elapsed_s"])
+    best = np.inf
+    running = []
+    t_train = time.time()
+    onestep_until = int(cfg.get("onestep_frac", 0.0) * cfg["steps"])
+    for step in range(1, cfg["steps"] + 1):
+        lr = corr.cosine_lr(step, cfg["steps"], cfg["lr"], min(cfg["warmup"], cfg["steps"] // 2))
+        # curriculum: one-step training first, so that the self-fed steps of the pushforward start from
+        # a model whose own rollouts are close to the data (the reference fine-tunes with --init); then
+        # pushforward steps alternate with one-step steps, which keep the one-step map anchored
+        pushforward = step > onestep_until and (step % 2 == 0 or not cfg.get("mix_onestep", True))
+        running.append(tr.step(lr, unroll=None if pushforward else 1))
+        if step % cfg["eval_every"] == 0 or step == cfg["steps"]:
+            tl = float(torch.stack(running).mean())
+            running = []
+            vh, vc = tr.evaluate(val_U)
+            row = [step, tl, vh, vc, vh / vc, lr, time.time() - t0]
+            hist.append(row)
+            log(f"{step:>6} train {tl:.3e} val hybrid {vh:.3e} coarse {vc:.3e} ratio {vh / vc:.3f} lr {lr:.2e} "
+                f"|g| {float(tr.net.norm):.2e} partial corrections {tr.fallback_count}/{4 * tr.B} "
+                f"{(time.time() - t_train) / step * 1e3:.2f} ms/step")
+            if writer:
+                writer.writerow(row)
+                logf.flush()
+            if out and vh < best:
+                best = vh
+                np.savez(out / "best.npz", params=tr.net.params.cpu().numpy(), stats=tr.stats.cpu().numpy(),
+                         dscale=tr.dscale.cpu().numpy())
+    tr.net.check_device_error()
+    if out:
+        np.savez(out / "last.npz", params=tr.net.params.cpu().numpy(), stats=tr.stats.cpu().numpy(),
+                 dscale=tr.dscale.cpu().numpy())
+        logf.close()
+    return tr, hist
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--out", default="runs/correction")
+    ap.add_argument("--n-traj", type=int, default=512)
+    ap.add_argument("--n-val", type=int, default=32)
+    ap.add_argument("--fine", type=int, default=512)
+    ap.add_argument("--coarse", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--unroll", type=int, default=4)
+    ap.add_argument("--onestep-frac", type=float, default=0.5,
+                    help="fraction of the steps trained one-step before the pushforward unroll starts")
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--warmup", type=int, default=500)
+    ap.add_argument("--eval-every", type=int, default=500)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    cfg = {k.replace("-", "_"): v for k, v in vars(a).items()}
+    train(cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -11,7 +11,7 @@ ROOT = Path(__file__).resolve().parents[1]
 PKG = ROOT / "neural-pde-surrogate_b200"
 
 # header -> shared library that implements it
-LIBS = {"fv.h": "libfv.so"}
+LIBS = {"fv.h": "libfv.so", "fvnet.h": "libfv.so"}
 
 
 def declared(header):
