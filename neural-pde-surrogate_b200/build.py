@@ -6,6 +6,8 @@ repository snapshot).  Cross-compiles for sm_100a with nvcc; no GPU needed to bu
 libfv.so -- the finite-volume solver (csrc/fv_api.cu + csrc/fv_kernels.cuh), C-ABI in include/fv.h.
             Built with --fmad=false: no FMA contraction, which keeps every result bit-identical to
             the reference CPU solver (its build uses none either).
+host/euler2d -- the reference's euler2d driver (main2d.cpp) over libfv.so's C-ABI, built with g++
+            -ffp-contract=off (its host-side to_primitive for snapshots must round like the reference).
 """
 import subprocess
 import sys
@@ -50,6 +52,15 @@ def build(force=False, verbose=False):
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         built.append(name)
+    exe, src = PKG / "host" / "euler2d", [PKG / "host" / "euler2d.cpp", PKG / "host" / "npz_io.hpp"]
+    if force or not exe.exists() or any(f.stat().st_mtime > exe.stat().st_mtime
+                                        for f in src + [PKG / "libfv.so", ROOT / "include" / "fv.h"]):
+        cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'include'}", "-o", str(exe), str(src[0]),
+               f"-L{PKG}", "-lfv", "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        built.append("host/euler2d")
     return built
 
 

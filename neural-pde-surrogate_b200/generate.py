@@ -6,6 +6,10 @@ reads the HDF5 trajectory back.  Here the same steps are one in-process call thr
 (fv_set_primitive + fv_run_trajectory): no subprocess, no files, the frames stay in memory.
 
   python neural-pde-surrogate_b200/generate.py --family blast --indices 0-7 --n 512 --save 128,64 --out DIR
+  torchrun --nproc-per-node 8 neural-pde-surrogate_b200/generate.py ...   (one GPU per rank)
+
+Under torchrun every rank takes a cost-balanced share of the indices (shard.balanced_split) and runs
+it on its own GPU; only the per-rank counts are gathered at the end (gloo, no data-path collective).
 
 Output per trajectory: DIR/<family>/<index:06d>.npz with `t` (frames,) and `U_<m>` (frames, 4, m, m)
 float32 conserved variables per save size, plus the run attributes the reference stores
@@ -85,14 +89,30 @@ def main():
     ap.add_argument("--out", required=True)
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
+    import torch
+    shard = importlib.import_module("neural-pde-surrogate_b200.shard")
+    ic = importlib.import_module("neural-pde-surrogate_b200.ic")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("gloo", timeout=datetime.timedelta(minutes=30))
     fv = importlib.import_module("neural-pde-surrogate_b200")
     save = [int(s) for s in a.save.split(",")]
     solver = fv.Solver(fv.make_grid(a.n, a.n, 0.0, 1.0, 0.0, 1.0, "periodic", "periodic"), "hllc", "vanleer", 0.5)
-    counts = {"done": 0, "skipped": 0}
+    indices = parse_indices(a.indices)
+    costs = []
+    for i in indices:
+        _, _, _, _, t_end, params = ic.sample(a.family, i, 8)
+        costs.append(shard.trajectory_cost(a.n, t_end - float(params.get("t_start", 0.0))))
     t0 = time.time()
-    for i in parse_indices(a.indices):
-        counts[generate_one(a.family, i, a.n, save, a.out, a.force, solver)] += 1
-    print(f"Finished in {time.time() - t0:.1f} s: {counts['done']} done, {counts['skipped']} skipped")
+    status = shard.run_sharded(indices, lambda i: generate_one(a.family, i, a.n, save, a.out, a.force, solver),
+                               costs=costs)
+    if status is not None:
+        print(f"Finished in {time.time() - t0:.1f} s: {status.count('done')} done, {status.count('skipped')} skipped"
+              f" on {world} GPU(s)")
+    if world > 1:
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
