@@ -76,6 +76,13 @@ const std::vector<TileVariant>& variants() {
         VariantMaker<64, 8, 512, 2>::make(),   // 3
         VariantMaker<32, 4, 128, 7>::make(),   // 4
         VariantMaker<16, 16, 288, 3>::make(),  // 5: 544 faces over 288 threads -> < 2 rounds
+        // shapes whose tile counts fill whole waves (4 x 148 or 2 x 148 resident CTAs) at 512^2 and
+        // 256^2, with faces and slopes in two rounds of the CTA's threads
+        VariantMaker<16, 14, 256, 4>::make(),  // 6: 512^2 -> 32 x 37 = 1184 tiles = 2 waves of 592
+        VariantMaker<32, 14, 512, 2>::make(),  // 7: 512^2 -> 16 x 37 = 592 tiles = 2 waves of 296
+        VariantMaker<16, 7, 128, 8>::make(),   // 8: 256^2 -> 16 x 37 = 592 tiles, 8 CTAs per SM
+        VariantMaker<16, 14, 256, 5>::make(),  // 9: 40 warps per SM at <= 51 registers
+        VariantMaker<16, 7, 128, 9>::make(),   // 10: 36 warps per SM at <= 56 registers
     };
     return v;
 }

@@ -59,7 +59,9 @@ __global__ void __launch_bounds__(NT, MINB) ensemble_stage_kernel(const GridDesc
         if (s_go) {
             double sx = 0.0, sy = 0.0;
             int bad = INT_MAX;
-            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, tile.i0, tile.j0, s_dt, s, sx, sy, bad);
+            // control ran before the load here: tiles of members that reached their target are skipped
+            // without loading anything
+            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, tile.i0, tile.j0, s_dt, s_go, [] {}, s, sx, sy, bad);
             if constexpr (STAGE == 2) {
                 reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
                 if (tile.leader && threadIdx.x == 0) c->step = c->step + 1;

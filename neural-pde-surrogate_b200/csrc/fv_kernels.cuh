@@ -176,9 +176,12 @@ __device__ __forceinline__ bool stage1_control(FvCtrl* c, const GridDesc& g, boo
 
 // The stage computation of one tile.  STAGE 1: U1 = U + dt L(U).  STAGE 2: U = 0.5 ((U + U1) +
 // dt L(U1)), plus the wave speeds of the new U into (sx, sy, bad).
-template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT>
-__device__ __forceinline__ void tile_body(const GridDesc& g, int i0, int j0, double dt, TileSmem<TX, TY>& s,
-                                          double& sx, double& sy, int& bad) {
+// Step control overlaps the halo load: every thread calls ctl() after issuing its P1 loads (one
+// thread does the work and fills the shared `go` and `dt`), and the P1 barrier publishes them.  dt is
+// read only in P4.  Returns false (for the whole CTA) when the grid does not step.
+template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, class Ctl>
+__device__ __forceinline__ bool tile_body(const GridDesc& g, int i0, int j0, const double& dt, const int& go, Ctl ctl,
+                                          TileSmem<TX, TY>& s, double& sx, double& sy, int& bad) {
     using S = TileSmem<TX, TY>;
     constexpr int HX = S::HX, HY = S::HY;
     constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
@@ -194,7 +197,9 @@ __device__ __forceinline__ void tile_body(const GridDesc& g, int i0, int j0, dou
         const int gj = bc_index(j0 - 2 + r, ny, g.bc_y);
         sts(s.W, r, col, ldg_q4(Win + (size_t)gj * nx + gi));
     }
+    ctl();
     __syncthreads();
+    if (!go) return false;
     FV_PHASE_MARK(1);
 
     // P2: limited slopes
@@ -270,6 +275,7 @@ __device__ __forceinline__ void tile_body(const GridDesc& g, int i0, int j0, dou
             wave_speed_cell(wn, (int)idx, sx, sy, bad);
         }
     }
+    return true;
 }
 
 // Single-grid stage kernel: grid (ceil(nx/TX), ceil(ny/TY)), one tile per CTA.
@@ -281,7 +287,9 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(GridDesc g) {
     __shared__ int s_go, s_par2;
     FvCtrl* c = g.ctrl;
     const bool leader = (blockIdx.x == 0 && blockIdx.y == 0);
-    if (threadIdx.x == 0) {
+    // the last thread has the fewest halo loads: it runs the step control while the others load
+    auto ctl = [&]() {
+        if (threadIdx.x != NT - 1) return;
         double dt;
         int go, par2 = 0;
         if constexpr (STAGE == 1) {
@@ -292,12 +300,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(GridDesc g) {
             par2 = c->par2;
         }
         s_go = go; s_dt = dt; s_par2 = par2;
-    }
-    __syncthreads();
-    if (!s_go) return;
+    };
     double sx = 0.0, sy = 0.0;
     int bad = INT_MAX;
-    tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, blockIdx.x * TX, blockIdx.y * TY, s_dt, s, sx, sy, bad);
+    if (!tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, blockIdx.x * TX, blockIdx.y * TY, s_dt, s_go, ctl, s, sx, sy, bad))
+        return;
     if constexpr (STAGE == 2) {
         reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
         if (leader && threadIdx.x == 0) c->step = c->step + 1;

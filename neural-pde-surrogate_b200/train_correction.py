@@ -173,7 +173,8 @@ def train(cfg, log=print):
                                                      indent=2))
         logf = open(out / "log.csv", "w", newline="")
         writer = csv.writer(logf)
-        writer.writerow(["step", "train_loss", "val_hybrid", "val_coarse", "val_ratio", "lr", "elapsed_s"])
+        writer.writerow(["step", "train_loss", "val_hybrid", "val_coarse", "val_ratio", "lr", "elapsed_s",
+                         "val_ratio_k"])
     best = np.inf
     running = []
     t_train = time.time()
@@ -189,16 +190,19 @@ def train(cfg, log=print):
             tl = float(torch.stack(running).mean())
             running = []
             vh, vc = tr.evaluate(val_U)
-            row = [step, tl, vh, vc, vh / vc, lr, time.time() - t0]
+            # model selection on k-step rollouts (k = select_k) when asked: what a pushforward model is for
+            k = int(cfg.get("select_k", 1))
+            kh, kc = tr.evaluate(val_U, batches=2, k=k) if k > 1 else (vh, vc)
+            row = [step, tl, vh, vc, vh / vc, lr, time.time() - t0, kh / kc]
             hist.append(row)
-            log(f"{step:>6} train {tl:.3e} val hybrid {vh:.3e} coarse {vc:.3e} ratio {vh / vc:.3f} lr {lr:.2e} "
-                f"|g| {float(tr.net.norm):.2e} partial corrections {tr.fallback_count}/{4 * tr.B} "
-                f"{(time.time() - t_train) / step * 1e3:.2f} ms/step")
+            log(f"{step:>6} train {tl:.3e} val hybrid {vh:.3e} coarse {vc:.3e} ratio {vh / vc:.3f} "
+                f"{k}-step ratio {kh / kc:.3f} lr {lr:.2e} |g| {float(tr.net.norm):.2e} partial corrections "
+                f"{tr.fallback_count}/{2 * k * tr.B} {(time.time() - t_train) / step * 1e3:.2f} ms/step")
             if writer:
                 writer.writerow(row)
                 logf.flush()
-            if out and vh < best:
-                best = vh
+            if out and kh / kc < best:
+                best = kh / kc
                 np.savez(out / "best.npz", params=tr.net.params.cpu().numpy(), stats=tr.stats.cpu().numpy(),
                          dscale=tr.dscale.cpu().numpy())
     tr.net.check_device_error()
@@ -225,6 +229,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=500)
     ap.add_argument("--eval-every", type=int, default=500)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--select-k", type=int, default=1,
+                    help="keep as best.npz the model with the lowest k-step validation ratio (hybrid / coarse)")
     a = ap.parse_args()
     cfg = {k.replace("-", "_"): v for k, v in vars(a).items()}
     train(cfg)

@@ -152,7 +152,7 @@ def _oracle(g, flux="hllc", limiter="vanleer"):
 def _to_primitive(U):  # state2d.hpp:21-25 in numpy (no FMA): same bits as the driver's snapshot writer
     u = U[..., 1] / U[..., 0]
     v = U[..., 2] / U[..., 0]
-    p = 0.4 * (U[..., 3] - 0.5 * U[..., 0] * (u * u + v * v))
+    p = (1.4 - 1.0) * (U[..., 3] - 0.5 * U[..., 0] * (u * u + v * v))  # GAMMA - 1.0, not 0.4
     return U[..., 0], u, v, p
 
 
