@@ -23,7 +23,7 @@ using namespace fv;
 
 namespace {
 
-constexpr int TX = 16, TY = 16, NT = 256, MINB = 4;  // the shape the autotuner picks for 256^2-512^2
+constexpr int TX = 16, TY = 14, NT = 256, MINB = 4;  // faces and slopes in two rounds of 256 threads
 using Smem = TileSmem<TX, TY>;
 
 struct Tile {

@@ -23,26 +23,36 @@
 #ifndef FV_PHASE_MARK
 #define FV_PHASE_MARK(k)
 #endif
+// Loop hint for the face phase (e.g. _Pragma("unroll 2") to let one thread's two faces interleave);
+// empty by default.
+#ifndef FV_FACE_LOOP_HINT
+#define FV_FACE_LOOP_HINT
+#endif
 
 namespace fv {
 
+// Shared-memory tile: every 4-vector field is two planes of double2, (q0, q1) and (q2, q3), so a Q4
+// moves with two 16-byte accesses and consecutive cells of a warp hit consecutive 16-byte words
+// (conflict-free).
 template <int TX_, int TY_>
 struct TileSmem {
     static constexpr int TX = TX_, TY = TY_, HX = TX + 4, HY = TY + 4;
-    double W[4][HY][HX];        // primitives of the tile + 2-cell halo
-    double dX[4][TY][TX + 2];   // x-slopes of cells -1..TX
-    double dY[4][TY + 2][TX];   // y-slopes of rows -1..TY
-    double F[4][TY][TX + 1];    // x-face fluxes
-    double G[4][TY + 1][TX];    // y-face fluxes
+    double2 W[2][HY][HX];        // primitives of the tile + 2-cell halo
+    double2 dX[2][TY][TX + 2];   // x-slopes of cells -1..TX
+    double2 dY[2][TY + 2][TX];   // y-slopes of rows -1..TY
+    double2 F[2][TY][TX + 1];    // x-face fluxes
+    double2 G[2][TY + 1][TX];    // y-face fluxes
 };
 
 template <int R, int Cc>
-__device__ __forceinline__ Q4 lds(const double (&a)[4][R][Cc], int r, int c) {
-    return Q4{a[0][r][c], a[1][r][c], a[2][r][c], a[3][r][c]};
+__device__ __forceinline__ Q4 lds(const double2 (&a)[2][R][Cc], int r, int c) {
+    const double2 lo = a[0][r][c], hi = a[1][r][c];
+    return Q4{lo.x, lo.y, hi.x, hi.y};
 }
 template <int R, int Cc>
-__device__ __forceinline__ void sts(double (&a)[4][R][Cc], int r, int c, const Q4& q) {
-    a[0][r][c] = q.a; a[1][r][c] = q.b; a[2][r][c] = q.c; a[3][r][c] = q.d;
+__device__ __forceinline__ void sts(double2 (&a)[2][R][Cc], int r, int c, const Q4& q) {
+    a[0][r][c] = make_double2(q.a, q.b);
+    a[1][r][c] = make_double2(q.c, q.d);
 }
 
 enum : int { MODE_LOOP = 0, MODE_FIXED = 1 };
@@ -217,6 +227,7 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, int i0, int j0, con
     FV_PHASE_MARK(2);
 
     // P3: face fluxes, flux(to_conserved(edge(W_L, dW_L, +1)), to_conserved(edge(W_R, dW_R, -1)))
+    FV_FACE_LOOP_HINT
     for (int e = threadIdx.x; e < NFX + NFY; e += NT) {
         Q4 wl, dl, wr, dr;
         const bool ydir = e >= NFX;

@@ -71,12 +71,23 @@ def l1_density(U, T):
     return (U[..., 0] - T[..., 0]).abs().sum(dim=(1, 2)) / (c * c)
 
 
+def by_family(L1, families):
+    """{family: mean L1 at the last frame} for per-sample L1 (B, frames)."""
+    if not families:
+        return {}
+    out = {}
+    for fam in sorted(set(families)):
+        idx = [k for k, f in enumerate(families) if f == fam]
+        out[fam] = round(float(L1[idx, -1].mean()), 5)
+    return out
+
+
 def drift(U, U0):
     """(total - total0) / sum |U0| per sample and field (rollout.py:54-62)."""
     return (U.sum(dim=(1, 2)) - U0.sum(dim=(1, 2))) / U0.abs().sum(dim=(1, 2))
 
 
-def run_plain(first, n, coarse, frames, truth):
+def run_plain(first, n, coarse, frames, truth, families=None):
     """All test trajectories at n^2 in one fv_ensemble; errors on the coarse grid."""
     import torch
     fv = importlib.import_module(PKG)
@@ -103,21 +114,23 @@ def run_plain(first, n, coarse, frames, truth):
         l1.append(l1_density(block_avg(U, n // coarse), truth[:, k]))
     L1 = torch.stack(l1, dim=1)
     return {"method": "plain", "n": n, "L1_final": float(L1[:, -1].mean()), "L1_mean": float(L1.mean()),
+            "L1_final_by_family": by_family(L1, families),
             "L1_per_frame": [round(float(v), 5) for v in L1.mean(dim=0)],
             "ms_per_traj": ms / B, "drift_mass": float(drift(U, first)[:, 0].abs().max()),
             "drift_energy": float(drift(U, first)[:, 3].abs().max()), "failed": int((status != 0).sum())}
 
 
-def run_hybrid(model, first, coarse, frames, truth, mode="scale"):
+def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, families=None):
     """mode: positivity rule of the correction ('strict': a step that would go non-physical is the plain
-    coarse step; 'scale': the largest physical fraction of the correction)."""
+    coarse step; 'scale': the largest physical fraction of the correction).  gain: a fixed factor on
+    every correction (1 = as trained)."""
     import torch
     corr = importlib.import_module(f"{PKG}.correction")
     z = np.load(model)
     B = first.shape[0]
     net = corr.CorrectionNet(B, coarse, coarse, params=z["params"])
     stats = torch.from_numpy(z["stats"]).cuda()
-    dscale = torch.from_numpy(z["dscale"]).cuda()
+    dscale = torch.from_numpy(z["dscale"]).cuda() * gain
     cs = corr.CoarseSolver(B, coarse, coarse)
     x = first.clone()
     Uc, Un = torch.empty_like(x), torch.empty_like(x)
@@ -137,7 +150,8 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale"):
         x.copy_(Un)
         l1.append(l1_density(x, truth[:, k]))
     L1 = torch.stack(l1, dim=1)
-    return {"method": f"hybrid-{mode}", "n": coarse, "L1_final": float(L1[:, -1].mean()), "L1_mean": float(L1.mean()),
+    return {"method": f"hybrid-{mode}" + (f"-g{gain:g}" if gain != 1.0 else ""), "n": coarse, "gain": gain,
+            "L1_final_by_family": by_family(L1, families), "L1_final": float(L1[:, -1].mean()), "L1_mean": float(L1.mean()),
             "L1_per_frame": [round(float(v), 5) for v in L1.mean(dim=0)], "mean_theta": float(np.mean(theta)),
             "ms_per_traj": ms / B, "drift_mass": float(drift(x, first)[:, 0].abs().max()),
             "drift_energy": float(drift(x, first)[:, 3].abs().max()), "fallback_steps": fallbacks}
@@ -154,12 +168,16 @@ def main():
     ap.add_argument("--kh", type=int, default=4)
     ap.add_argument("--plain", default="64,128,256,512")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--gains", default="1", help="comma-separated correction gains to evaluate (scale mode)")
     a = ap.parse_args()
     plain = [int(x) for x in a.plain.split(",")]
     items = test_set(a.riemann, a.blast, a.kh)
     truth, first = truth_frames(items, a.truth, a.coarse, a.frames, sorted(set(plain + [a.coarse])))
-    hybrids = [run_hybrid(a.model, first[a.coarse], a.coarse, a.frames, truth, mode) for mode in ("scale", "strict")]
-    plains = [run_plain(first[n], n, a.coarse, a.frames, truth) for n in plain]
+    gains = [float(g) for g in a.gains.split(",")]
+    fams = [f for f, _ in items]
+    hybrids = [run_hybrid(a.model, first[a.coarse], a.coarse, a.frames, truth, "scale", g, fams) for g in gains]
+    hybrids.append(run_hybrid(a.model, first[a.coarse], a.coarse, a.frames, truth, "strict", families=fams))
+    plains = [run_plain(first[n], n, a.coarse, a.frames, truth, fams) for n in plain]
     rows = hybrids + plains
     summary = {"test_set": {"riemann": a.riemann, "blast": a.blast, "kh": a.kh}, "truth": a.truth, "frames": a.frames,
                "rows": rows, "equal_error": {}}
@@ -172,11 +190,11 @@ def main():
                                                      "speedup": best["ms_per_traj"] / hyb["ms_per_traj"]}
         else:
             summary["equal_error"][hyb["method"]] = None
-    print(f"{'method':14s} {'n':>5s} {'L1 final':>10s} {'L1 mean':>10s} {'ms/traj':>9s} {'drift m':>9s} {'drift E':>9s}"
-          f" {'partial':>8s}")
+    print(f"{'method':18s} {'n':>5s} {'L1 final':>10s} {'L1 mean':>10s} {'ms/traj':>9s} {'drift m':>9s} {'drift E':>9s}"
+          f" {'partial':>8s}  L1 final by family")
     for r in rows:
-        print(f"{r['method']:14s} {r['n']:5d} {r['L1_final']:10.3e} {r['L1_mean']:10.3e} {r['ms_per_traj']:9.2f} "
-              f"{r['drift_mass']:9.1e} {r['drift_energy']:9.1e} {r.get('fallback_steps', r.get('failed', 0)):8d}")
+        print(f"{r['method']:18s} {r['n']:5d} {r['L1_final']:10.3e} {r['L1_mean']:10.3e} {r['ms_per_traj']:9.2f} "
+              f"{r['drift_mass']:9.1e} {r['drift_energy']:9.1e} {r.get('fallback_steps', r.get('failed', 0)):8d}  {r['L1_final_by_family']}")
     print(json.dumps(summary))
     if a.out:
         Path(a.out).write_text(json.dumps(summary, indent=2))

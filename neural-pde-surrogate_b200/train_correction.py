@@ -86,7 +86,7 @@ def residual_scale(U, coarse_solver, B, rng, pairs=4):
 
 
 class Trainer:
-    def __init__(self, train, val, batch, unroll, seed=0, log=print):
+    def __init__(self, train, val, batch, unroll, seed=0, log=print, init=None):
         import torch
         self.torch = torch
         corr = importlib.import_module(f"{PKG}.correction")
@@ -96,9 +96,15 @@ class Trainer:
         H, W = train.shape[2:4]
         self.rng = np.random.default_rng(seed)
         self.coarse = corr.CoarseSolver(batch, H, W)
-        self.net = corr.CorrectionNet(batch, H, W, seed=seed)
-        self.stats = field_stats(train)
-        self.dscale = residual_scale(train, self.coarse, batch, self.rng)
+        if init is None:
+            self.net = corr.CorrectionNet(batch, H, W, seed=seed)
+            self.stats = field_stats(train)
+            self.dscale = residual_scale(train, self.coarse, batch, self.rng)
+        else:  # fine-tuning (train.py --init): the checkpoint's parameters and its normalisation
+            z = np.load(init)
+            self.net = corr.CorrectionNet(batch, H, W, params=z["params"])
+            self.stats = torch.from_numpy(z["stats"]).cuda()
+            self.dscale = torch.from_numpy(z["dscale"]).cuda()
         shape = (batch, H, W, 4)
         self.x = torch.empty(shape, dtype=torch.float64, device="cuda")
         self.Uc = torch.empty_like(self.x)
@@ -106,6 +112,7 @@ class Trainer:
         self.fb = torch.zeros(batch, dtype=torch.int32, device="cuda")
         self.loss_part = torch.zeros(batch, dtype=torch.float64, device="cuda")
         self.mode = "scale"  # positivity rule of the self-fed and evaluation steps
+        self.noise = 0.0     # relative input noise of the trained step (set by train())
         log(f"stats mean {self.stats[:4].tolist()} std {(1 / self.stats[4:]).tolist()}; "
             f"residual scale {self.dscale.tolist()}")
 
@@ -124,6 +131,8 @@ class Trainer:
             self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un,
                                   self.fb, mode=self.mode)
             self.x.copy_(self.Un)
+        if self.noise > 0.0:
+            self.perturb(self.x, self.noise)
         # the trained step keeps its full correction even where it is non-physical: the loss then pulls
         # it toward the (physical) target instead of the sample dropping out of the gradient
         self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un, self.fb,
@@ -132,6 +141,26 @@ class Trainer:
         self.net.backward()
         self.net.adamw(lr)
         return self.loss_part.sum() / (self.B * self.Un[0].numel())
+
+    def perturb(self, x, sigma):
+        """Noise injection (in place): the input frame of a training pair gets relative noise of size
+        sigma in rho and p and velocity noise of sigma times the local sound speed, in primitive
+        variables so that the state stays physical; the target stays the clean next frame, so the
+        network also learns to pull perturbed states back (a stand-in for its own rollout errors)."""
+        torch = self.torch
+        rho = x[..., 0]
+        u, v = x[..., 1] / rho, x[..., 2] / rho
+        p = (1.4 - 1.0) * (x[..., 3] - 0.5 * rho * (u * u + v * v))
+        c = torch.sqrt(1.4 * p / rho)
+        g = torch.randn_like(x)
+        rho = rho * torch.exp(sigma * g[..., 0])
+        p = p * torch.exp(sigma * g[..., 3])
+        u = u + sigma * c * g[..., 1]
+        v = v + sigma * c * g[..., 2]
+        x[..., 0] = rho
+        x[..., 1] = rho * u
+        x[..., 2] = rho * v
+        x[..., 3] = p / (1.4 - 1.0) + 0.5 * rho * (u * u + v * v)
 
     def evaluate(self, U, batches=4, k=1, mode=None):
         """Mean normalised MSE after k steps of (hybrid, coarse-only) on pairs drawn from U."""
@@ -163,7 +192,8 @@ def train(cfg, log=print):
     t0 = time.time()
     train_U = build_dataset(cfg["n_traj"], cfg["fine"], cfg["coarse"], index0=0, log=log)
     val_U = build_dataset(cfg["n_val"], cfg["fine"], cfg["coarse"], index0=100000, log=log)
-    tr = Trainer(train_U, val_U, cfg["batch"], cfg["unroll"], seed=cfg["seed"], log=log)
+    tr = Trainer(train_U, val_U, cfg["batch"], cfg["unroll"], seed=cfg["seed"], log=log, init=cfg.get("init"))
+    tr.noise = float(cfg.get("noise", 0.0))
     corr = tr.corr
     hist = []
     writer = None
@@ -229,6 +259,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=500)
     ap.add_argument("--eval-every", type=int, default=500)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--init", default=None, help="start from this checkpoint (params, stats, dscale)")
+    ap.add_argument("--noise", type=float, default=0.0,
+                    help="relative noise injected into the trained step's input (0 = none)")
     ap.add_argument("--select-k", type=int, default=1,
                     help="keep as best.npz the model with the lowest k-step validation ratio (hybrid / coarse)")
     a = ap.parse_args()
