@@ -148,16 +148,16 @@ def run_ours(args):
     def device_step(k):
         """One bench step with resident inputs; returns cell-updates."""
         cells = 0
-        with torch.cuda.stream(stream):
+        with torch.cuda.stream(stream):  # the solvers' stream: device buffers need no cross-stream ordering
             flush.zero_()
-        for s in solvers:
-            s.set_state(dev_U[k])
-            for fr in range(NOUT + 1):
-                if fr:
-                    _, nst = s.advance_to(0.0 + (T_END - 0.0) * fr / NOUT)
-                for m in SAVE:
-                    s.block_average(n // m, out=dev_out[m][fr])
-            cells += n * n * s.time()[1]
+            for s in solvers:
+                s.set_state(dev_U[k])
+                for fr in range(NOUT + 1):
+                    if fr:
+                        _, nst = s.advance_to(0.0 + (T_END - 0.0) * fr / NOUT)
+                    for m in SAVE:
+                        s.block_average(n // m, out=dev_out[m][fr])
+                cells += n * n * s.time()[1]
         return cells
 
     def e2e_step(k):

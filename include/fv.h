@@ -138,6 +138,8 @@ int fv_ensemble_state_device(fv_ensemble* e, int member, double** dU);
  * others continue, and the call then returns FV_ERR_NONPHYSICAL. */
 int fv_ensemble_advance_to(fv_ensemble* e, const double* t_next, double* t, long long* steps, int* status);
 int fv_ensemble_launch_count(fv_ensemble* e, long long* launches);
+/* The ensemble's cudaStream_t (see fv_get_stream). */
+int fv_ensemble_get_stream(fv_ensemble* e, void** stream);
 
 /* Face fluxes of n face pairs evaluated on the GPU by the same device code the stage kernels use:
  * the FluxFn (riemann2d.hpp:8; rusanov_flux :11-15, hllc_flux :27-39) for y_face = 0, or
@@ -190,6 +192,13 @@ int fv_launch_count(fv_solver* s, long long* launches);
 
 /* Blocks until all work queued on the handle's stream is done. */
 int fv_synchronize(fv_solver* s);
+
+/* The cudaStream_t the handle's work is queued on (the one given to fv_create, or the library's own
+ * non-blocking stream).  The *_device entry points read and write caller memory in this stream's
+ * order: a caller that produces or consumes those buffers on another stream orders the two streams
+ * itself (events), e.g. the Python mirror against torch's current stream.  No reference counterpart
+ * (the reference is CPU code). */
+int fv_get_stream(fv_solver* s, void** stream);
 
 /* Message for the calling thread's last failing call ("" if none). */
 const char* fv_last_error(void);

@@ -50,6 +50,8 @@ _PROTOS = {
     "fv_block_average_device": [_P, _I, _P],
     "fv_run_trajectory": [_P, _D, _D, _I, _P, _I, _P, _P, _LLP, _BP],
     "fv_synchronize": [_P],
+    "fv_get_stream": [_P, C.POINTER(C.c_void_p)],
+    "fv_ensemble_get_stream": [_P, C.POINTER(C.c_void_p)],
     "fv_riemann_flux": [_I, _I, _I, _P, _P, _P],
     "fv_fill_ghosts": [_I, _I, _I, _I, _P, _P],
     "fv_profile": [_P, _I],
@@ -84,6 +86,35 @@ _PROTOS = {
 }
 
 _lib = None
+
+
+class StreamOrder:
+    """Orders a library handle's CUDA stream against torch's current stream.  The library queues the
+    *_device copies on its own non-blocking stream, which nothing orders against torch's work: a
+    tensor written by torch must be complete before the library reads it (before()), and torch must
+    not read what the library writes until it is done (after())."""
+
+    def __init__(self, getter, handle):
+        p = C.c_void_p()
+        check(getter(handle, C.byref(p)))
+        self.ptr = p.value or 0
+        self._ext = None
+
+    def _streams(self):
+        import torch
+        if self._ext is None:
+            self._ext = torch.cuda.ExternalStream(self.ptr) if self.ptr else torch.cuda.default_stream()
+        return torch.cuda.current_stream(), self._ext
+
+    def before(self):
+        cur, ext = self._streams()
+        if ext != cur:
+            ext.wait_stream(cur)
+
+    def after(self):
+        cur, ext = self._streams()
+        if ext != cur:
+            cur.wait_stream(ext)
 
 
 def lib():

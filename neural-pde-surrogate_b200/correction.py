@@ -204,7 +204,9 @@ class CoarseSolver:
 def hybrid_step(net, coarse, U, dt_frame, stats, dscale, Uc, Unext, fallback, mode="scale"):
     """One hybrid step: Uc = coarse(U, dt_frame); Unext = Uc + projected correction under the
     positivity rule `mode` ('strict': fall back to the plain coarse step; 'scale': largest physical
-    fraction of the correction; 'keep': full correction)."""
+    fraction of the correction; 'keep': full correction).  Returns the coarse solve's (steps, status):
+    status[b] != 0 means sample b's coarse step stopped at a non-physical state before dt_frame, so
+    its Uc and Unext are not states at the new time -- callers must not use them as such."""
     steps, status = coarse.advance(U, dt_frame, Uc)
     net.correct(Uc, stats, dscale, Unext, fallback, mode)
     return steps, status

@@ -709,4 +709,10 @@ int fv_synchronize(fv_solver* s) {
     return FV_OK;
 }
 
+int fv_get_stream(fv_solver* s, void** stream) {
+    if (!s || !stream) return set_error(FV_ERR_ARG, "fv_get_stream: NULL argument");
+    *stream = static_cast<void*>(s->stream);
+    return FV_OK;
+}
+
 }  // extern "C"

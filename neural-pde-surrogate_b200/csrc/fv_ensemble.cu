@@ -395,4 +395,10 @@ int fv_ensemble_launch_count(fv_ensemble* e, long long* n) {
     return FV_OK;
 }
 
+int fv_ensemble_get_stream(fv_ensemble* e, void** stream) {
+    if (!e || !stream) return err(FV_ERR_ARG, "fv_ensemble_get_stream: bad arguments");
+    *stream = static_cast<void*>(e->stream);
+    return FV_OK;
+}
+
 }  // extern "C"

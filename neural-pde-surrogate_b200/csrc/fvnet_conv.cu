@@ -234,25 +234,35 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
         uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
         for (int e = tid; e < W * OC; e += NT) Ds4[e] = a.dZ[size_t(n * H + y) * W * OC + e];
         __syncthreads();
-        // A[kc][m = shift*CIN + ci] = X[y+ky-1][kc*8 + i + kx - 1][ci], i = 0..7 (periodic)
-        for (int e = tid; e < KC * M9; e += NT) {
-            const int m = e % M9, kc = e / M9;
-            const int sh = m / CIN, ci = m % CIN, ky = sh / 3, kx = sh % 3;
-            float v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int x = (kc * 8 + i + kx - 1 + W) % W;
-                v[i] = __bfloat162float(Xs[(ky * W + x) * CIN + ci]);
+        // A[kc][m = shift*CIN + ci] = X[y+ky-1][kc*8 + i + kx - 1][ci], i = 0..7 (periodic), and
+        // B[kc][co] = dZ[kc*8 + i][co]: 8x8 bf16 transposes, four per warp instruction pair.  Lane l
+        // names row l%8 of matrix l/8: ldmatrix.trans reads 8 pixel rows (16 bytes = 8 channels each)
+        // and stmatrix writes them back as 8 channel rows of 8 pixels -- one K-major core-matrix row
+        // each.
+        {
+            const int r8 = lane & 7, mq = lane >> 3;
+            constexpr int NA = 9 * CC;  // matrices per kc for A
+            const int na = KC * NA, nb = KC * OC;
+            const uint32_t xsb = tc::smem_addr(Xs), dsb = tc::smem_addr(Ds);
+            for (int q0 = warp * 4; q0 < na + nb; q0 += 4 * (NT / 32)) {
+                const int q = q0 + mq;
+                uint32_t src, dst;
+                if (q < na) {
+                    const int kc = q / NA, rest = q - kc * NA, sh = rest / CC, cc = rest - sh * CC;
+                    const int ky = sh / 3, kx = sh - ky * 3;
+                    int xs = kc * 8 + r8 + kx - 1;
+                    xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
+                    src = xsb + uint32_t(((ky * W + xs) * CIN + cc * 8) * 2);
+                    dst = ab + uint32_t((kc * MROWS + sh * CIN + cc * 8 + r8) * 16);
+                } else {
+                    const int qb = q - na, kc = qb / OC, oc = qb - kc * OC;
+                    src = dsb + uint32_t(((kc * 8 + r8) * COUT + oc * 8) * 2);
+                    dst = bb + uint32_t((kc * COUT + oc * 8 + r8) * 16);
+                }
+                uint32_t v0, v1, v2, v3;
+                tc::ldsm_x4_trans(src, v0, v1, v2, v3);
+                tc::stsm_x4(dst, v0, v1, v2, v3);
             }
-            As[size_t(kc) * MROWS + m] = pack8(v);
-        }
-        // B[kc][co] = dZ[kc*8 + i][co]
-        for (int e = tid; e < KC * COUT; e += NT) {
-            const int co = e % COUT, kc = e / COUT;
-            float v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = __bfloat162float(Ds[(kc * 8 + i) * COUT + co]);
-            Bs[e] = pack8(v);
         }
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
@@ -433,7 +443,7 @@ int fvnet_conv3x3(int mode, int cin_pad, int cout_pad, int B, int H, int W, cons
     return FVNET_OK;
 }
 
-int fvnet_wgrad_parts(int B, int H) { return std::max(1, std::min(148, B * H)); }
+int fvnet_wgrad_parts(int B, int H) { return std::max(1, std::min(2 * 148, B * H)); }  // 2 CTAs per SM at W <= 64
 
 int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int H, int W, const void* X, const void* dZ,
                         float* partial, float* dW, float* db, float* db_part, int* err, void* stream) {

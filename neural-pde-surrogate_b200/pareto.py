@@ -134,14 +134,28 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, fami
     cs = corr.CoarseSolver(B, coarse, coarse)
     x = first.clone()
     Uc, Un = torch.empty_like(x), torch.empty_like(x)
+    Uc_prev, Uc2 = first.clone(), torch.empty_like(x)
     fb = torch.zeros(B, dtype=torch.int32, device="cuda")
     corr.hybrid_step(net, cs, x.clone(), 1e-9, stats, dscale, Uc, Un, fb, mode)  # warm-up (kernel loading)
     torch.cuda.synchronize()
-    l1, ms, fallbacks, theta = [], 0.0, 0, []
+    l1, ms, fallbacks, theta, retried, failed = [], 0.0, 0, [], 0, 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for k in range(1, frames + 1):
         e0.record()
-        corr.hybrid_step(net, cs, x, DT_FRAME, stats, dscale, Uc, Un, fb, mode)
+        _, status = corr.hybrid_step(net, cs, x, DT_FRAME, stats, dscale, Uc, Un, fb, mode)
+        bad = np.nonzero(status)[0]
+        if len(bad):
+            # the coarse solver cannot advance these corrected states: drop the previous frame's
+            # correction (restart from its uncorrected coarse state) and take a plain coarse step
+            retried += len(bad)
+            idx = torch.as_tensor(bad, device="cuda")
+            x2 = x.clone()
+            x2[idx] = Uc_prev[idx]
+            _, st2 = cs.advance(x2, DT_FRAME, Uc2)
+            Uc[idx] = Uc2[idx]
+            Un[idx] = Uc2[idx]
+            failed += int((st2[bad] != 0).sum())
+        Uc_prev.copy_(Uc)
         e1.record()
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
@@ -154,7 +168,8 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, fami
             "L1_final_by_family": by_family(L1, families), "L1_final": float(L1[:, -1].mean()), "L1_mean": float(L1.mean()),
             "L1_per_frame": [round(float(v), 5) for v in L1.mean(dim=0)], "mean_theta": float(np.mean(theta)),
             "ms_per_traj": ms / B, "drift_mass": float(drift(x, first)[:, 0].abs().max()),
-            "drift_energy": float(drift(x, first)[:, 3].abs().max()), "fallback_steps": fallbacks}
+            "drift_energy": float(drift(x, first)[:, 3].abs().max()), "fallback_steps": fallbacks,
+            "coarse_retries": retried, "failed": failed}
 
 
 def main():
@@ -191,10 +206,11 @@ def main():
         else:
             summary["equal_error"][hyb["method"]] = None
     print(f"{'method':18s} {'n':>5s} {'L1 final':>10s} {'L1 mean':>10s} {'ms/traj':>9s} {'drift m':>9s} {'drift E':>9s}"
-          f" {'partial':>8s}  L1 final by family")
+          f" {'partial':>8s} {'retries':>7s}  L1 final by family")
     for r in rows:
         print(f"{r['method']:18s} {r['n']:5d} {r['L1_final']:10.3e} {r['L1_mean']:10.3e} {r['ms_per_traj']:9.2f} "
-              f"{r['drift_mass']:9.1e} {r['drift_energy']:9.1e} {r.get('fallback_steps', r.get('failed', 0)):8d}  {r['L1_final_by_family']}")
+              f"{r['drift_mass']:9.1e} {r['drift_energy']:9.1e} {r.get('fallback_steps', r.get('failed', 0)):8d} "
+              f"{r.get('coarse_retries', 0):7d}  {r['L1_final_by_family']}")
     print(json.dumps(summary))
     if a.out:
         Path(a.out).write_text(json.dumps(summary, indent=2))

@@ -19,7 +19,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import BadCell, check, lib
+from ._lib import BadCell, StreamOrder, check, lib
 
 FLUXES = {"rusanov": 0, "hllc": 1}            # main2d.cpp:145-148
 LIMITERS = {"none": 0, "unlimited": 1, "minmod": 2, "vanleer": 3}  # main2d.cpp:150-155
@@ -112,12 +112,18 @@ class Solver:
         """U: host ndarray (ny, nx, 4) float64, or a CUDA torch tensor of that shape."""
         if hasattr(U, "data_ptr") and getattr(U, "is_cuda", False):
             assert tuple(U.shape) == self.shape and U.is_contiguous() and str(U.dtype) == "torch.float64"
+            self._order().before()
             check(lib().fv_set_state_device(self._h, _dev_ptr(U)))
             return
         U = np.ascontiguousarray(U, dtype=np.float64)
         if U.shape != self.shape:
             raise ValueError(f"state must have shape {self.shape}, got {U.shape}")
         check(lib().fv_set_state(self._h, _ptr(U)))
+
+    def _order(self):
+        if getattr(self, "_stream_order", None) is None:
+            self._stream_order = StreamOrder(lib().fv_get_stream, self._h)
+        return self._stream_order
 
     def set_primitive(self, rho, u, v, p):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, v, p)]
@@ -128,7 +134,9 @@ class Solver:
 
     def get_state(self, out=None):
         if out is not None and hasattr(out, "data_ptr") and getattr(out, "is_cuda", False):
+            self._order().before()
             check(lib().fv_get_state_device(self._h, _dev_ptr(out)))
+            self._order().after()
             return out
         out = np.empty(self.shape, np.float64) if out is None else out
         check(lib().fv_get_state(self._h, _ptr(out)))
@@ -172,7 +180,9 @@ class Solver:
         """trajectory.hpp:31-51 for one level: (4, ny/f, nx/f) float32."""
         shape = (4, self.grid.ny // factor, self.grid.nx // factor)
         if out is not None and hasattr(out, "data_ptr") and getattr(out, "is_cuda", False):
+            self._order().before()
             check(lib().fv_block_average_device(self._h, int(factor), _dev_ptr(out)))
+            self._order().after()
             return out
         out = np.empty(shape, np.float32) if out is None else out
         check(lib().fv_block_average(self._h, int(factor), _ptr(out)))

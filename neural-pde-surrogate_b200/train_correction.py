@@ -111,6 +111,8 @@ class Trainer:
         self.Un = torch.empty_like(self.x)
         self.fb = torch.zeros(batch, dtype=torch.int32, device="cuda")
         self.loss_part = torch.zeros(batch, dtype=torch.float64, device="cuda")
+        self.ok = torch.ones(batch, dtype=torch.float64, device="cuda")
+        self.coarse_failures = 0
         self.mode = "scale"  # positivity rule of the self-fed and evaluation steps
         self.noise = 0.0     # relative input noise of the trained step (set by train())
         log(f"stats mean {self.stats[:4].tolist()} std {(1 / self.stats[4:]).tolist()}; "
@@ -127,17 +129,24 @@ class Trainer:
         unroll = unroll or self.unroll
         x, y = self._pairs(self.train_U, unroll)
         self.x.copy_(x)
-        for _ in range(unroll - 1):  # self-fed steps, no gradient, physical by construction
-            self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un,
-                                  self.fb, mode=self.mode)
+        ok = np.ones(self.B, bool)  # samples whose coarse steps all reached the frame time
+        for _ in range(unroll - 1):  # self-fed steps, no gradient
+            _, status = self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc,
+                                              self.Un, self.fb, mode=self.mode)
+            ok &= status == 0
             self.x.copy_(self.Un)
         if self.noise > 0.0:
             self.perturb(self.x, self.noise)
         # the trained step keeps its full correction even where it is non-physical: the loss then pulls
         # it toward the (physical) target instead of the sample dropping out of the gradient
-        self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un, self.fb,
-                              mode="keep")
-        self.net.loss_grad(self.Un, y, self.Uc, self.stats, self.dscale, None, self.loss_part)
+        _, status = self.corr.hybrid_step(self.net, self.coarse, self.x, DT_FRAME, self.stats, self.dscale, self.Uc,
+                                          self.Un, self.fb, mode="keep")
+        ok &= status == 0
+        # a sample whose coarse solve stopped early (a self-fed state the solver cannot advance) has no
+        # state at the target time: it gets no gradient (theta 0)
+        self.coarse_failures += int((~ok).sum())
+        self.ok.copy_(self.torch.from_numpy(ok.astype(np.float64)))
+        self.net.loss_grad(self.Un, y, self.Uc, self.stats, self.dscale, None if ok.all() else self.ok, self.loss_part)
         self.net.backward()
         self.net.adamw(lr)
         return self.loss_part.sum() / (self.B * self.Un[0].numel())
@@ -167,19 +176,25 @@ class Trainer:
         h, c = 0.0, 0.0
         inv = self.stats[4:]
         self.fallback_count = 0
+        self.eval_failures = 0
         for _ in range(batches):
             x, y = self._pairs(U, k)
             xh = x.clone()
             xc = x.clone()
+            ok = np.ones(self.B, bool)
             for _ in range(k):
-                self.corr.hybrid_step(self.net, self.coarse, xh, DT_FRAME, self.stats, self.dscale, self.Uc, self.Un,
-                                      self.fb, mode=mode or self.mode)
+                _, status = self.corr.hybrid_step(self.net, self.coarse, xh, DT_FRAME, self.stats, self.dscale, self.Uc,
+                                                  self.Un, self.fb, mode=mode or self.mode)
+                ok &= status == 0
                 self.fallback_count += int(self.fb.sum())
                 xh.copy_(self.Un)
                 self.coarse.advance(xc, DT_FRAME, self.Uc)
                 xc.copy_(self.Uc)
-            h += float((((xh - y) * inv) ** 2).mean())
-            c += float((((xc - y) * inv) ** 2).mean())
+            self.eval_failures += int((~ok).sum())
+            keep = self.torch.from_numpy(ok).cuda()
+            if keep.any():  # samples whose hybrid coarse solve stopped early are counted, not scored
+                h += float((((xh[keep] - y[keep]) * inv) ** 2).mean())
+                c += float((((xc[keep] - y[keep]) * inv) ** 2).mean())
         return h / batches, c / batches
 
 
@@ -227,7 +242,8 @@ def train(cfg, log=print):
             hist.append(row)
             log(f"{step:>6} train {tl:.3e} val hybrid {vh:.3e} coarse {vc:.3e} ratio {vh / vc:.3f} "
                 f"{k}-step ratio {kh / kc:.3f} lr {lr:.2e} |g| {float(tr.net.norm):.2e} partial corrections "
-                f"{tr.fallback_count}/{2 * k * tr.B} {(time.time() - t_train) / step * 1e3:.2f} ms/step")
+                f"{tr.fallback_count}/{2 * k * tr.B} coarse failures: eval {tr.eval_failures}/{2 * tr.B} train "
+                f"{tr.coarse_failures} {(time.time() - t_train) / step * 1e3:.2f} ms/step")
             if writer:
                 writer.writerow(row)
                 logf.flush()

@@ -104,3 +104,29 @@ def test_nonphysical_member_stops_alone():
     assert steps[0] == ns and bits_equal(ens.get_state(0), Us) and bits_equal(ens.get_state(2), Us)
     with pytest.raises(fv.FVError):
         ens.advance_to(0.3)
+
+
+def test_device_buffers_are_ordered_against_torchs_stream():
+    """The ensemble queues its copies on its own non-blocking stream.  A tensor whose last write on
+    torch's current stream is still queued behind a long matmul must still reach the ensemble intact
+    (set_all waits for torch's stream), and torch must see get_all's copy (it waits for the library's
+    stream) -- without either wait the copy would move stale data."""
+    import torch
+    B, n = 4, 64
+    g = fv.make_grid(n, n, 0.0, 1.0, 0.0, 1.0, "periodic", "periodic")
+    e = ens_mod.Ensemble([g] * B, "hllc", "vanleer")
+    U = torch.stack([torch.from_numpy(ic.to_conserved(*ic.sample("riemann", k, n)[:4])) for k in range(B)]).cuda()
+    x = torch.zeros_like(U)
+    big = torch.randn(6144, 6144, device="cuda")
+    out = torch.zeros_like(U)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        y = big @ big  # milliseconds of queued work on torch's stream
+        x.copy_(U + 0.0 * y[0, 0].double())  # x is final only after the matmul
+        e.set_all(x)
+        e.get_all(out)
+        res = out * 1.0  # torch work on out, queued right behind get_all
+        torch.cuda.synchronize()
+        assert torch.equal(res, U)
+        x.zero_()
+        out.zero_()
