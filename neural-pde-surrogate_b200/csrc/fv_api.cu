@@ -42,7 +42,7 @@ int set_error(int code, const char* fmt, ...) {
                              __LINE__);                                                                \
     } while (0)
 
-using StageFn = void (*)(GridDesc);
+using StageFn = void (*)(GridDesc, TileMaps);
 
 // Tile shapes the stage kernels are instantiated for.  All give bit-identical results; the
 // autotuner (fv_autotune) picks the fastest for a grid.  MINB = CTAs per SM the launch bounds ask
@@ -111,6 +111,8 @@ struct fv_solver {
     float* d_avg = nullptr;
     size_t d_avg_cap = 0;
     int variant = 0;          // tile shape (index into variants())
+    TileMaps maps{};          // TMA descriptors of W, W1 for the tile shape maps_variant
+    int maps_variant = -1;
     bool tuned = false;       // variant chosen by the autotuner or fixed by fv_set_tile
     bool has_state = false;
     long long launches = 0;  // kernels launched by this handle
@@ -150,14 +152,50 @@ int retire_oldest(fv_solver* s) {
     return FV_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link to libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// TMA descriptors of g's primitive arrays (two planes of nx*ny double2 each) for a (tx+4) x (ty+4)
+// halo box.  use = 0 when the driver offers no encoder (every tile then takes the BC-mapped load).
+int encode_maps(const GridDesc& g, int tx, int ty, TileMaps* out) {
+    *out = TileMaps{};
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return FV_OK;
+    const cuuint64_t dims[4] = {2, (cuuint64_t)g.nx, (cuuint64_t)g.ny, 2};
+    const cuuint64_t strides[3] = {16, 16ull * g.nx, 16ull * g.nx * g.ny};  // bytes, dims 1..3
+    const cuuint32_t box[4] = {2, (cuuint32_t)(tx + 4), (cuuint32_t)(ty + 4), 2};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    for (int k = 0; k < 2; ++k) {
+        CUresult r = fn(k == 0 ? &out->w : &out->w1, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, k == 0 ? (void*)g.W : (void*)g.W1,
+                        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_error(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    }
+    out->use = 1;
+    return FV_OK;
+}
+
 // Enqueues stage 1 and stage 2 of one step of grid g with tile variant v.
-int enqueue_step(const GridDesc& g, int v, int flux, int lim, cudaStream_t st, cudaEvent_t* ev) {
+int enqueue_step(const GridDesc& g, const TileMaps& tm, int v, int flux, int lim, cudaStream_t st, cudaEvent_t* ev) {
     const TileVariant& tv = variants()[v];
     const dim3 grid((g.nx + tv.tx - 1) / tv.tx, (g.ny + tv.ty - 1) / tv.ty);
     if (ev) FV_CUDA(cudaEventRecord(ev[0], st));
-    tv.s1[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g);
+    tv.s1[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g, tm);
     if (ev) FV_CUDA(cudaEventRecord(ev[1], st));
-    tv.s2[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g);
+    tv.s2[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g, tm);
     if (ev) FV_CUDA(cudaEventRecord(ev[2], st));
     FV_CUDA(cudaGetLastError());
     return FV_OK;
@@ -193,7 +231,13 @@ int launch_step(fv_solver* s) {
         s->ring_used++;
     }
     s->launches += 2;
-    return enqueue_step(s->desc(), s->variant, s->flux, s->lim, s->stream, ev);
+    if (s->maps_variant != s->variant) {
+        const TileVariant& tv = variants()[s->variant];
+        int rc = encode_maps(s->desc(), tv.tx, tv.ty, &s->maps);
+        if (rc) return rc;
+        s->maps_variant = s->variant;
+    }
+    return enqueue_step(s->desc(), s->maps, s->variant, s->flux, s->lim, s->stream, ev);
 }
 
 int read_ctrl(fv_solver* s) {
@@ -272,10 +316,12 @@ int autotune(fv_solver* s, int steps, int* chosen) {
         if (e != cudaSuccess) break;
         ctrl_reset_kernel<<<1, 1, 0, s->stream>>>(ct, 0.0, 1);
         ctrl_set_kernel<<<1, 1, 0, s->stream>>>(ct, MODE_FIXED, 0.0, dt);
-        for (int k = 0; k < 2 && rc == FV_OK; ++k) rc = enqueue_step(g, v, s->flux, s->lim, s->stream, nullptr);
+        TileMaps tm;
+        if ((rc = encode_maps(g, variants()[v].tx, variants()[v].ty, &tm))) break;
+        for (int k = 0; k < 2 && rc == FV_OK; ++k) rc = enqueue_step(g, tm, v, s->flux, s->lim, s->stream, nullptr);
         if (rc) break;
         if ((e = cudaEventRecord(e0, s->stream)) != cudaSuccess) break;
-        for (int k = 0; k < steps && rc == FV_OK; ++k) rc = enqueue_step(g, v, s->flux, s->lim, s->stream, nullptr);
+        for (int k = 0; k < steps && rc == FV_OK; ++k) rc = enqueue_step(g, tm, v, s->flux, s->lim, s->stream, nullptr);
         if (rc) break;
         if ((e = cudaEventRecord(e1, s->stream)) != cudaSuccess) break;
         if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
@@ -524,6 +570,7 @@ int fv_advance_to(fv_solver* s, double t_next, double* t_out, long long* steps_o
         return set_error(FV_ERR_NONPHYSICAL, "Non-physical state in cell (%d, %d)", c.bad_index % s->nx,
                          c.bad_index / s->nx);
     }
+    if (c.status == FV_ERR_TIMEOUT) return set_error(FV_ERR_TIMEOUT, "fv_advance_to: a tile's TMA load did not land");
     return FV_OK;
 }
 

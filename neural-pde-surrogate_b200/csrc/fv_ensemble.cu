@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(NT, MINB) ensemble_stage_kernel(const GridDesc
             int bad = INT_MAX;
             // control ran before the load here: tiles of members that reached their target are skipped
             // without loading anything
-            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, tile.i0, tile.j0, s_dt, s_go, [] {}, s, sx, sy, bad);
+            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, nullptr, tile.i0, tile.j0, s_dt, s_go, [] {}, s, sx, sy, bad);
             if constexpr (STAGE == 2) {
                 reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
                 if (tile.leader && threadIdx.x == 0) c->step = c->step + 1;

@@ -11,13 +11,18 @@
 //       (solver2d.hpp:141,149-150,176-177), then the stage update (solver2d.hpp:92 / :100).
 //       Stage 2 also reduces the next step's CFL wave speeds and the first non-physical cell
 //       (compute_dt, solver2d.hpp:67-83) into the control block: dt never leaves the device.
-// Shared memory is structure-of-arrays (one plane per variable) so that a warp reading 32
-// consecutive cells touches 32 consecutive doubles: no bank conflicts.
+// The primitive arrays W, W1 are stored in HBM as two planes of double2, (rho, u) and (v, p), the
+// layout of the shared-memory tile: an interior tile's halo block is one TMA box (P1), boundary tiles
+// load cell by cell through the BC index map.
 // Every face flux is computed from the same inputs in the same order whatever the tile shape, so all
 // tile shapes give bit-identical results; the shape is a tuning choice (fv_autotune).
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include <climits>
+
 #include "fv_physics.cuh"
+#include "tc_sm100.cuh"
 
 // Phase marker inside tile_body (no-op unless a build defines it, e.g. to record clock64()).
 #ifndef FV_PHASE_MARK
@@ -42,6 +47,7 @@ struct TileSmem {
     double2 dY[2][TY + 2][TX];   // y-slopes of rows -1..TY
     double2 F[2][TY][TX + 1];    // x-face fluxes
     double2 G[2][TY + 1][TX];    // y-face fluxes
+    uint64_t bar;                // mbarrier of the P1 TMA load
 };
 
 template <int R, int Cc>
@@ -72,7 +78,7 @@ struct FvCtrl {
     double dt_fixed;               // dt of fv_step
     long long step;                // steps taken
     int mode;
-    int status;                    // 0, or FV_ERR_NONPHYSICAL
+    int status;                    // 0, FV_ERR_NONPHYSICAL, or FV_ERR_TIMEOUT (a bounded wait ran out)
     int bad_index;                 // row-major index recorded with status
     int pad_;
 };
@@ -91,6 +97,27 @@ struct GridDesc {
     double cx, cy;    // 1.0/dx and 1.0/dy, as the reference writes (1.0 / g.dx)
     FvCtrl* ctrl;
 };
+
+// TMA descriptors of one grid's W and W1 for one tile shape: 4-D (2 doubles, nx, ny, 2 planes) with
+// box (2, TX + 4, TY + 4, 2) -- a tile's halo block of both planes.  Passed to the single-grid stage
+// kernel as a __grid_constant__ parameter (a TMA descriptor must live in parameter, constant or
+// global memory).
+struct TileMaps {
+    CUtensorMap w, w1;
+    int use;  // 0: every tile loads through the BC index map
+};
+
+// Primitive arrays: plane 0 = (rho, u), plane 1 = (v, p), each n = nx * ny cells of double2.
+__device__ __forceinline__ Q4 ldg_w(const Q4* W, size_t n, size_t k) {
+    const double2* p = reinterpret_cast<const double2*>(W);
+    const double2 lo = __ldg(p + k), hi = __ldg(p + n + k);
+    return Q4{lo.x, lo.y, hi.x, hi.y};
+}
+__device__ __forceinline__ void st_w(Q4* W, size_t n, size_t k, const Q4& q) {
+    double2* p = reinterpret_cast<double2*>(W);
+    p[k] = make_double2(q.a, q.b);
+    p[n + k] = make_double2(q.c, q.d);
+}
 
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
@@ -190,25 +217,48 @@ __device__ __forceinline__ bool stage1_control(FvCtrl* c, const GridDesc& g, boo
 // thread does the work and fills the shared `go` and `dt`), and the P1 barrier publishes them.  dt is
 // read only in P4.  Returns false (for the whole CTA) when the grid does not step.
 template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, class Ctl>
-__device__ __forceinline__ bool tile_body(const GridDesc& g, int i0, int j0, const double& dt, const int& go, Ctl ctl,
-                                          TileSmem<TX, TY>& s, double& sx, double& sy, int& bad) {
+__device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm, int i0, int j0, const double& dt,
+                                          const int& go, Ctl ctl, TileSmem<TX, TY>& s, double& sx, double& sy,
+                                          int& bad) {
     using S = TileSmem<TX, TY>;
     constexpr int HX = S::HX, HY = S::HY;
     constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
     constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
     const int nx = g.nx, ny = g.ny;
+    const size_t ncell = (size_t)nx * ny;
     const Q4* __restrict__ Win = (STAGE == 1) ? g.W : g.W1;
 
     FV_PHASE_MARK(0);
-    // P1: primitives of the halo tile (solver2d.hpp:133-134 on the ghost-filled array)
-    for (int e = threadIdx.x; e < HX * HY; e += NT) {
-        const int r = e / HX, col = e - r * HX;
-        const int gi = bc_index(i0 - 2 + col, nx, g.bc_x);
-        const int gj = bc_index(j0 - 2 + r, ny, g.bc_y);
-        sts(s.W, r, col, ldg_q4(Win + (size_t)gj * nx + gi));
+    // P1: primitives of the halo tile (solver2d.hpp:133-134 on the ghost-filled array).  A tile whose
+    // halo lies inside the grid is one TMA box, issued by one thread; a tile at the grid's edge maps
+    // every halo cell through the BC.
+    const bool tma = tm != nullptr && tm->use && i0 >= 2 && j0 >= 2 && i0 + TX + 2 <= nx && j0 + TY + 2 <= ny &&
+                     (tc::smem_addr(&s.W[0][0][0]) & 127u) == 0;  // the copy's destination alignment
+    if (tma) {
+        if (threadIdx.x == 0) {
+            tc::mbar_init(&s.bar, 1);
+            tc::fence_mbar_init();
+            tc::mbar_arrive_expect_tx(&s.bar, (uint32_t)sizeof(s.W));
+            tc::tma_load_4d(&s.W[0][0][0], (STAGE == 1) ? (const void*)&tm->w : (const void*)&tm->w1, 0, i0 - 2,
+                            j0 - 2, 0, &s.bar);
+        }
+    } else {
+        for (int e = threadIdx.x; e < HX * HY; e += NT) {
+            const int r = e / HX, col = e - r * HX;
+            const int gi = bc_index(i0 - 2 + col, nx, g.bc_x);
+            const int gj = bc_index(j0 - 2 + r, ny, g.bc_y);
+            sts(s.W, r, col, ldg_w(Win, ncell, (size_t)gj * nx + gi));
+        }
     }
     ctl();
     __syncthreads();
+    if (tma) {  // every thread waits (bounded); the CTA leaves as a whole if any wait ran out
+        const int lost = tc::mbar_wait_bounded(&s.bar, 0, nullptr) ? 0 : 1;
+        if (__syncthreads_or(lost)) {
+            if (threadIdx.x == 0) atomicExch(&g.ctrl->status, 4);  // FV_ERR_TIMEOUT: the grid stops
+            return false;
+        }
+    }
     if (!go) return false;
     FV_PHASE_MARK(1);
 
@@ -274,7 +324,7 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, int i0, int j0, con
             const Q4 u = ldg_q4(g.U + idx);
             const Q4 u1{u.a + dt * L.a, u.b + dt * L.b, u.c + dt * L.c, u.d + dt * L.d};
             st_q4(g.U1 + idx, u1);
-            st_q4(g.W1 + idx, to_primitive(u1));
+            st_w(g.W1, ncell, idx, to_primitive(u1));
         } else {
             const Q4 u = ld_q4(g.U + idx);
             const Q4 u1 = ldg_q4(g.U1 + idx);
@@ -282,7 +332,7 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, int i0, int j0, con
                         0.5 * (u.c + u1.c + dt * L.c), 0.5 * (u.d + u1.d + dt * L.d)};
             const Q4 wn = to_primitive(un);
             st_q4(g.U + idx, un);
-            st_q4(g.W + idx, wn);
+            st_w(g.W, ncell, idx, wn);
             wave_speed_cell(wn, (int)idx, sx, sy, bad);
         }
     }
@@ -291,8 +341,8 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, int i0, int j0, con
 
 // Single-grid stage kernel: grid (ceil(nx/TX), ceil(ny/TY)), one tile per CTA.
 template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) stage_kernel(GridDesc g) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const __grid_constant__ TileMaps tm) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destination: 128-byte aligned
     auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
     __shared__ double s_dt;
     __shared__ int s_go, s_par2;
@@ -314,7 +364,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(GridDesc g) {
     };
     double sx = 0.0, sy = 0.0;
     int bad = INT_MAX;
-    if (!tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, blockIdx.x * TX, blockIdx.y * TY, s_dt, s_go, ctl, s, sx, sy, bad))
+    if (!tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, &tm, blockIdx.x * TX, blockIdx.y * TY, s_dt, s_go, ctl, s, sx, sy,
+                                                 bad))
         return;
     if constexpr (STAGE == 2) {
         reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
@@ -332,7 +383,7 @@ static __global__ void __launch_bounds__(RED_NT) wave_speed_kernel(const Q4* __r
     int bad = INT_MAX;
     for (int k = blockIdx.x * RED_NT + threadIdx.x; k < n; k += gridDim.x * RED_NT) {
         const Q4 w = to_primitive(ldg_q4(U + k));
-        st_q4(W + k, w);
+        st_w(W, (size_t)n, k, w);
         wave_speed_cell(w, k, sx, sy, bad);
     }
     reduce_wave_speeds<RED_NT>(sx, sy, bad, c, par);

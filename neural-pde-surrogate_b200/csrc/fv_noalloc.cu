@@ -44,7 +44,7 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_dev_ptr[kMaxDevices] = {};
 
-using StageFn = void (*)(GridDesc);
+using StageFn = void (*)(GridDesc, TileMaps);
 
 template <int F, int L>
 void pick(StageFn* s1, StageFn* s2) {
@@ -133,8 +133,9 @@ extern "C" int fv_step_noalloc(int nx, int ny, double x_min, double x_max, doubl
     ctrl_reset_kernel<<<1, 1, 0, st>>>(g.ctrl, 0.0, 1);
     ctrl_set_kernel<<<1, 1, 0, st>>>(g.ctrl, MODE_FIXED, 0.0, dt);
     wave_speed_kernel<<<std::max(1, std::min((n + RED_NT - 1) / RED_NT, 148 * 8)), RED_NT, 0, st>>>(g.U, g.W, n, g.ctrl);
-    s1<<<grid, NT, sizeof(TileSmem<TX, TY>), st>>>(g);
-    s2<<<grid, NT, sizeof(TileSmem<TX, TY>), st>>>(g);
+    const TileMaps no_tma{};  // every tile loads through the BC index map
+    s1<<<grid, NT, sizeof(TileSmem<TX, TY>), st>>>(g, no_tma);
+    s2<<<grid, NT, sizeof(TileSmem<TX, TY>), st>>>(g, no_tma);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fv_internal_set_error(FV_ERR_CUDA, cudaGetErrorString(e));
     return FV_OK;

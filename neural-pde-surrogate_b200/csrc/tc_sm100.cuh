@@ -40,6 +40,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase,
     return false;
 }
 
+// Arrive on the barrier and add `bytes` to the transaction count the current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// ---- TMA -----------------------------------------------------------------------------------------
+// One 4-D tiled box of the tensor map `tmap` (in kernel-parameter, constant or global memory) at
+// coordinates (c0, c1, c2, c3) into this CTA's shared memory at `dst`; completion is signalled on
+// `bar` as transaction bytes.  No multicast.  The innermost coordinate c0 times the element size must
+// be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0, int c1, int c2, int c3, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+        : "memory");
+}
+
 // ---- fences --------------------------------------------------------------------------------------
 // Generic-proxy shared-memory writes made visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

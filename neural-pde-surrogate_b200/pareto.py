@@ -196,21 +196,34 @@ def main():
     rows = hybrids + plains
     summary = {"test_set": {"riemann": a.riemann, "blast": a.blast, "kh": a.kh}, "truth": a.truth, "frames": a.frames,
                "rows": rows, "equal_error": {}}
-    for hyb in hybrids:  # the coarsest plain resolution at least as accurate as the hybrid, and its cost
-        cheaper = [r for r in plains if r["L1_final"] <= hyb["L1_final"]]
-        if cheaper:
-            best = min(cheaper, key=lambda r: r["n"])
-            summary["equal_error"][hyb["method"]] = {"plain_n": best["n"], "plain_ms": best["ms_per_traj"],
-                                                     "hybrid_ms": hyb["ms_per_traj"],
-                                                     "speedup": best["ms_per_traj"] / hyb["ms_per_traj"]}
-        else:
-            summary["equal_error"][hyb["method"]] = None
+    # equal error at several horizons: the coarsest plain resolution whose L1 at frame h is at most the
+    # hybrid's, and the cost ratio (frame costs are near constant, so whole-run times compare)
+    horizons = sorted({h for h in (5, 10, 20, a.frames) if h <= a.frames})
+    summary["horizons"] = horizons
+    for hyb in hybrids:
+        per = {}
+        for h in horizons:
+            e = hyb["L1_per_frame"][h - 1]
+            cheaper = [r for r in plains if r["L1_per_frame"][h - 1] <= e]
+            if cheaper:
+                best = min(cheaper, key=lambda r: r["n"])
+                per[h] = {"hybrid_L1": e, "plain_n": best["n"], "plain_L1": best["L1_per_frame"][h - 1],
+                          "plain_ms": best["ms_per_traj"], "hybrid_ms": hyb["ms_per_traj"],
+                          "speedup": best["ms_per_traj"] / hyb["ms_per_traj"]}
+            else:
+                per[h] = {"hybrid_L1": e, "plain_n": None}
+        summary["equal_error"][hyb["method"]] = per
     print(f"{'method':18s} {'n':>5s} {'L1 final':>10s} {'L1 mean':>10s} {'ms/traj':>9s} {'drift m':>9s} {'drift E':>9s}"
           f" {'partial':>8s} {'retries':>7s}  L1 final by family")
     for r in rows:
         print(f"{r['method']:18s} {r['n']:5d} {r['L1_final']:10.3e} {r['L1_mean']:10.3e} {r['ms_per_traj']:9.2f} "
               f"{r['drift_mass']:9.1e} {r['drift_energy']:9.1e} {r.get('fallback_steps', r.get('failed', 0)):8d} "
               f"{r.get('coarse_retries', 0):7d}  {r['L1_final_by_family']}")
+    for m, per in summary["equal_error"].items():
+        cells = []
+        for h, r in per.items():
+            cells.append(f"{h}: " + (f"plain {r['plain_n']} x{r['speedup']:.2f}" if r["plain_n"] else "none"))
+        print(f"equal error {m:18s} " + "; ".join(cells))
     print(json.dumps(summary))
     if a.out:
         Path(a.out).write_text(json.dumps(summary, indent=2))
