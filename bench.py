@@ -52,15 +52,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of the stage-2 kernel from the committed ncu summary, or None."""
+def profiled(key):
+    """A figure of the committed ncu summary of the stage kernels ("key: value" line), or None."""
     f = ROOT / "profiles" / "fv_stage_kernels_blast512.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch_stage2:"):
+        if line.startswith(key + ":"):
             return float(line.split(":")[1])
     return None
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the stage-2 kernel from the committed ncu summary, or None."""
+    return profiled("traffic_bytes_per_launch_stage2")
 
 
 class Clocks:
@@ -238,7 +243,9 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": f"stage_kernel<stage {stage}>", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_cell": STAGE_BYTES[stage],
-                     "mean_launch_ms": {"stage1": ms1, "stage2": ms2}},
+                     "mean_launch_ms": {"stage1": ms1, "stage2": ms2},
+                     # what binds instead: the FP64 pipe (ncu share of active cycles, committed summary)
+                     "fp64_pipe_active_ncu": profiled("fp64_pipe_active_stage2")},
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:

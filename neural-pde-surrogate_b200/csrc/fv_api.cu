@@ -352,6 +352,7 @@ bool valid_common(int flux, int lim, int bc_x, int bc_y) {
 
 // Lets the library's other translation units report through fv_last_error().
 int fv_internal_set_error(int code, const char* msg) { return set_error(code, "%s", msg ? msg : ""); }
+int fv_internal_encode_maps(const GridDesc& g, int tx, int ty, TileMaps* out) { return encode_maps(g, tx, ty, out); }
 
 extern "C" {
 

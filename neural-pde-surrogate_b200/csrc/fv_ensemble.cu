@@ -18,6 +18,7 @@
 #include "fv_kernels.cuh"
 
 int fv_internal_set_error(int code, const char* msg);
+int fv_internal_encode_maps(const fv::GridDesc& g, int tx, int ty, fv::TileMaps* out);
 
 using namespace fv;
 
@@ -34,11 +35,18 @@ struct Tile {
 // tile table.
 template <int FLUX, int LIM, int STAGE>
 __global__ void __launch_bounds__(NT, MINB) ensemble_stage_kernel(const GridDesc* __restrict__ members,
+                                                                  const TileMaps* __restrict__ maps,
                                                                   const Tile* __restrict__ tiles, int ntiles) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destination: 128-byte aligned
     Smem& s = *reinterpret_cast<Smem*>(smem_raw);
     __shared__ double s_dt;
     __shared__ int s_go, s_par2;
+    // one TMA barrier for all of the CTA's tiles, its phase tracked across them
+    if (maps != nullptr && threadIdx.x == 0) {
+        tc::mbar_init(&s.bar, 1);
+        tc::fence_mbar_init();
+    }
+    uint32_t phase = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const Tile tile = tiles[t];
         const GridDesc g = members[tile.member];
@@ -61,7 +69,8 @@ __global__ void __launch_bounds__(NT, MINB) ensemble_stage_kernel(const GridDesc
             int bad = INT_MAX;
             // control ran before the load here: tiles of members that reached their target are skipped
             // without loading anything
-            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, nullptr, tile.i0, tile.j0, s_dt, s_go, [] {}, s, sx, sy, bad);
+            tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, maps ? maps + tile.member : nullptr, phase, tile.i0, tile.j0,
+                                                   s_dt, s_go, [] {}, s, sx, sy, bad);
             if constexpr (STAGE == 2) {
                 reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
                 if (tile.leader && threadIdx.x == 0) c->step = c->step + 1;
@@ -79,7 +88,7 @@ __global__ void ensemble_set_kernel(FvCtrl* ctrl, const double* t_next, int coun
     ctrl[m].status = 0;
 }
 
-using StageFn = void (*)(const GridDesc*, const Tile*, int);
+using StageFn = void (*)(const GridDesc*, const TileMaps*, const Tile*, int);
 
 template <int F, int L>
 void pick(StageFn* s1, StageFn* s2) {
@@ -116,6 +125,7 @@ struct fv_ensemble {
     FvCtrl* ctrl = nullptr;
     FvCtrl* h_ctrl = nullptr;          // pinned mirror
     GridDesc* d_members = nullptr;
+    TileMaps* d_maps = nullptr;        // per member TMA descriptors of W, W1 for the ensemble's tile
     Tile* d_tiles = nullptr;
     int ntiles = 0;
     double* d_tnext = nullptr;
@@ -139,8 +149,8 @@ int err(int code, const char* msg) { return fv_internal_set_error(code, msg); }
 
 int enqueue_steps(fv_ensemble* e, int nsteps) {
     for (int k = 0; k < nsteps; ++k) {
-        e->s1<<<e->grid, NT, sizeof(Smem), e->stream>>>(e->d_members, e->d_tiles, e->ntiles);
-        e->s2<<<e->grid, NT, sizeof(Smem), e->stream>>>(e->d_members, e->d_tiles, e->ntiles);
+        e->s1<<<e->grid, NT, sizeof(Smem), e->stream>>>(e->d_members, e->d_maps, e->d_tiles, e->ntiles);
+        e->s2<<<e->grid, NT, sizeof(Smem), e->stream>>>(e->d_members, e->d_maps, e->d_tiles, e->ntiles);
     }
     EN_CUDA(cudaGetLastError());
     return FV_OK;
@@ -264,6 +274,18 @@ int fv_ensemble_create(int count, const int* nx, const int* ny, const double* bo
     }
     if (rc == FV_OK && (ce = cudaMemcpy(e->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice)) != cudaSuccess) fail(ce);
     if (rc == FV_OK && (ce = cudaMemcpy(e->d_members, e->h_members.data(), count * sizeof(GridDesc), cudaMemcpyHostToDevice)) != cudaSuccess) fail(ce);
+    if (rc == FV_OK) {  // TMA descriptors (left out when the driver offers no encoder)
+        std::vector<TileMaps> maps(count);
+        bool any = false;
+        for (int m = 0; m < count && rc == FV_OK; ++m) {
+            rc = fv_internal_encode_maps(e->h_members[m], TX, TY, &maps[m]);
+            any = any || maps[m].use;
+        }
+        if (rc == FV_OK && any) {
+            if ((ce = cudaMalloc(&e->d_maps, count * sizeof(TileMaps))) != cudaSuccess) fail(ce);
+            else if ((ce = cudaMemcpy(e->d_maps, maps.data(), count * sizeof(TileMaps), cudaMemcpyHostToDevice)) != cudaSuccess) fail(ce);
+        }
+    }
     for (StageFn f : {e->s1, e->s2})
         if (rc == FV_OK && (ce = cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem))) != cudaSuccess) fail(ce);
     if (rc != FV_OK) {
@@ -281,6 +303,7 @@ int fv_ensemble_destroy(fv_ensemble* e) {
     cudaFree(e->pool);
     cudaFree(e->ctrl);
     cudaFree(e->d_members);
+    cudaFree(e->d_maps);
     cudaFree(e->d_tiles);
     cudaFree(e->d_tnext);
     cudaFreeHost(e->h_ctrl);

@@ -216,10 +216,13 @@ __device__ __forceinline__ bool stage1_control(FvCtrl* c, const GridDesc& g, boo
 // Step control overlaps the halo load: every thread calls ctl() after issuing its P1 loads (one
 // thread does the work and fills the shared `go` and `dt`), and the P1 barrier publishes them.  dt is
 // read only in P4.  Returns false (for the whole CTA) when the grid does not step.
+// tm: the grid's TMA descriptors for this tile shape, or nullptr; s.bar must have been initialised
+// (count 1) by the caller, and `phase` is the barrier's next phase parity (flipped after every TMA
+// tile; CTA-uniform).
 template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, class Ctl>
-__device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm, int i0, int j0, const double& dt,
-                                          const int& go, Ctl ctl, TileSmem<TX, TY>& s, double& sx, double& sy,
-                                          int& bad) {
+__device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm, uint32_t& phase, int i0, int j0,
+                                          const double& dt, const int& go, Ctl ctl, TileSmem<TX, TY>& s, double& sx,
+                                          double& sy, int& bad) {
     using S = TileSmem<TX, TY>;
     constexpr int HX = S::HX, HY = S::HY;
     constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
@@ -236,8 +239,6 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
                      (tc::smem_addr(&s.W[0][0][0]) & 127u) == 0;  // the copy's destination alignment
     if (tma) {
         if (threadIdx.x == 0) {
-            tc::mbar_init(&s.bar, 1);
-            tc::fence_mbar_init();
             tc::mbar_arrive_expect_tx(&s.bar, (uint32_t)sizeof(s.W));
             tc::tma_load_4d(&s.W[0][0][0], (STAGE == 1) ? (const void*)&tm->w : (const void*)&tm->w1, 0, i0 - 2,
                             j0 - 2, 0, &s.bar);
@@ -253,7 +254,8 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
     ctl();
     __syncthreads();
     if (tma) {  // every thread waits (bounded); the CTA leaves as a whole if any wait ran out
-        const int lost = tc::mbar_wait_bounded(&s.bar, 0, nullptr) ? 0 : 1;
+        const int lost = tc::mbar_wait_bounded(&s.bar, phase, nullptr) ? 0 : 1;
+        phase ^= 1u;
         if (__syncthreads_or(lost)) {
             if (threadIdx.x == 0) atomicExch(&g.ctrl->status, 4);  // FV_ERR_TIMEOUT: the grid stops
             return false;
@@ -364,8 +366,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
     };
     double sx = 0.0, sy = 0.0;
     int bad = INT_MAX;
-    if (!tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, &tm, blockIdx.x * TX, blockIdx.y * TY, s_dt, s_go, ctl, s, sx, sy,
-                                                 bad))
+    if (tm.use && threadIdx.x == 0) {  // other threads touch the barrier only after the P1 barrier
+        tc::mbar_init(&s.bar, 1);
+        tc::fence_mbar_init();
+    }
+    uint32_t phase = 0;
+    if (!tile_body<FLUX, LIM, STAGE, TX, TY, NT>(g, &tm, phase, blockIdx.x * TX, blockIdx.y * TY, s_dt, s_go, ctl, s,
+                                                 sx, sy, bad))
         return;
     if constexpr (STAGE == 2) {
         reduce_wave_speeds<NT>(sx, sy, bad, c, s_par2);
