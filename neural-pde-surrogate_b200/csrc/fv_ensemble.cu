@@ -175,6 +175,57 @@ int read_ctrl(fv_ensemble* e) {
     return FV_OK;
 }
 
+// Every member at once (fv_ensemble_set_all_device): the control blocks reset in one launch, then
+// W = to_primitive(U) and the wave speeds / positivity of every member in one launch whose blockIdx.y
+// is the member -- instead of two launches per member.  Per member the work and the reduction are
+// those of ctrl_reset_kernel + wave_speed_kernel.
+__global__ void ensemble_reset_kernel(FvCtrl* ctrl, int count) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= count) return;
+    FvCtrl* c = ctrl + m;
+    c->step = 0;
+    c->sxy[0][0] = 0ull;
+    c->sxy[0][1] = 0ull;
+    c->bad[0] = INT_MAX;
+    c->t[0] = 0.0;
+    c->status = 0;
+    c->bad_index = -1;
+    c->run2 = 0;
+}
+__global__ void __launch_bounds__(RED_NT) ensemble_prime_kernel(const GridDesc* __restrict__ members) {
+    const GridDesc g = members[blockIdx.y];
+    const int n = g.nx * g.ny;
+    double sx = 0.0, sy = 0.0;
+    int bad = INT_MAX;
+    for (int k = blockIdx.x * RED_NT + threadIdx.x; k < n; k += gridDim.x * RED_NT) {
+        const Q4 w = to_primitive(ldg_q4(g.U + k));
+        st_w(g.W, (size_t)n, k, w);
+        wave_speed_cell(w, k, sx, sy, bad);
+    }
+    reduce_wave_speeds<RED_NT>(sx, sy, bad, g.ctrl, 0);
+}
+
+int prime_member(fv_ensemble* e, int m);
+
+int prime_all(fv_ensemble* e) {
+    if (e->count > 65535) {  // beyond gridDim.y: member by member
+        for (int m = 0; m < e->count; ++m) {
+            int rc = prime_member(e, m);
+            if (rc) return rc;
+        }
+        return FV_OK;
+    }
+    int maxn = 1;
+    for (const GridDesc& g : e->h_members) maxn = std::max(maxn, g.nx * g.ny);
+    ensemble_reset_kernel<<<(e->count + 127) / 128, 128, 0, e->stream>>>(e->ctrl, e->count);
+    const dim3 grid(std::max(1, std::min((maxn + RED_NT - 1) / RED_NT, 64)), e->count);
+    ensemble_prime_kernel<<<grid, RED_NT, 0, e->stream>>>(e->d_members);
+    e->launches += 2;
+    EN_CUDA(cudaGetLastError());
+    for (int m = 0; m < e->count; ++m) e->has_state[m] = 1;
+    return FV_OK;
+}
+
 int prime_member(fv_ensemble* e, int m) {
     const GridDesc& g = e->h_members[m];
     ctrl_reset_kernel<<<1, 1, 0, e->stream>>>(g.ctrl, 0.0, 1);
@@ -340,11 +391,7 @@ int fv_ensemble_get_state(fv_ensemble* e, int m, double* U) {
 int fv_ensemble_set_all_device(fv_ensemble* e, const double* dU) {
     if (!e || !dU) return err(FV_ERR_ARG, "fv_ensemble_set_all_device: bad arguments");
     EN_CUDA(cudaMemcpyAsync(e->pool, dU, e->total_cells * sizeof(Q4), cudaMemcpyDeviceToDevice, e->stream));
-    for (int m = 0; m < e->count; ++m) {
-        int rc = prime_member(e, m);
-        if (rc) return rc;
-    }
-    return FV_OK;
+    return prime_all(e);
 }
 
 int fv_ensemble_get_all_device(fv_ensemble* e, double* dU) {
