@@ -192,10 +192,22 @@ int encode_maps(const GridDesc& g, int tx, int ty, TileMaps* out) {
 int enqueue_step(const GridDesc& g, const TileMaps& tm, int v, int flux, int lim, cudaStream_t st, cudaEvent_t* ev) {
     const TileVariant& tv = variants()[v];
     const dim3 grid((g.nx + tv.tx - 1) / tv.tx, (g.ny + tv.ty - 1) / tv.ty);
+    // both stages as programmatic dependent launches: a stage's CTAs get resident while the previous
+    // kernel of the stream drains, and start the moment it completes (griddepcontrol.wait)
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(tv.nt);
+    cfg.dynamicSmemBytes = tv.smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;  // with events between the stages, each interval is completion to completion
     if (ev) FV_CUDA(cudaEventRecord(ev[0], st));
-    tv.s1[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g, tm);
+    FV_CUDA(cudaLaunchKernelEx(&cfg, tv.s1[flux][lim], g, tm));
     if (ev) FV_CUDA(cudaEventRecord(ev[1], st));
-    tv.s2[flux][lim]<<<grid, tv.nt, tv.smem, st>>>(g, tm);
+    FV_CUDA(cudaLaunchKernelEx(&cfg, tv.s2[flux][lim], g, tm));
     if (ev) FV_CUDA(cudaEventRecord(ev[2], st));
     FV_CUDA(cudaGetLastError());
     return FV_OK;

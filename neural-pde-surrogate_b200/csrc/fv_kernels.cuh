@@ -28,11 +28,6 @@
 #ifndef FV_PHASE_MARK
 #define FV_PHASE_MARK(k)
 #endif
-// Loop hint for the face phase (e.g. _Pragma("unroll 2") to let one thread's two faces interleave);
-// empty by default.
-#ifndef FV_FACE_LOOP_HINT
-#define FV_FACE_LOOP_HINT
-#endif
 
 namespace fv {
 
@@ -279,7 +274,6 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
     FV_PHASE_MARK(2);
 
     // P3: face fluxes, flux(to_conserved(edge(W_L, dW_L, +1)), to_conserved(edge(W_R, dW_R, -1)))
-    FV_FACE_LOOP_HINT
     for (int e = threadIdx.x; e < NFX + NFY; e += NT) {
         Q4 wl, dl, wr, dr;
         const bool ydir = e >= NFX;
@@ -348,6 +342,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
     auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
     __shared__ double s_dt;
     __shared__ int s_go, s_par2;
+    // Programmatic dependent launch: this grid may have been launched while the previous stage still
+    // runs; nothing below may touch its outputs before the wait (a no-op for a plain launch).  The
+    // next stage may launch once every CTA of this grid has started.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
     FvCtrl* c = g.ctrl;
     const bool leader = (blockIdx.x == 0 && blockIdx.y == 0);
     // the last thread has the fewest halo loads: it runs the step control while the others load
