@@ -169,6 +169,12 @@ int fv_tile_variant(int variant, int* tx, int* ty, int* threads);
 int fv_profile(fv_solver* s, int enable);
 int fv_profile_read(fv_solver* s, double* ms_stage1, double* ms_stage2, long long* steps_timed);
 
+/* Self-test of the library's bounded waits: runs the wait used for every TMA copy and tensor-core
+ * batch on a barrier that nothing arrives at, with a 10 ms limit.  Returns FV_ERR_TIMEOUT when the
+ * wait gave up and reported it (the expected outcome; the context stays usable), FV_ERR_STATE if it
+ * did not, FV_ERR_CUDA on a CUDA error.  No reference counterpart (the reference has no GPU code). */
+int fv_wait_selftest(void);
+
 /* Measured FP64 FMA throughput of the current device (DFMA per second, one FMA = 2 flops): the
  * denominator of the FP64-pipe roofline the stage kernels are reported against.  No reference
  * counterpart (the reference has no GPU code). */

@@ -22,8 +22,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 
 LIBS = {
     "libfv.so": {
-        "sources": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_ensemble.cu", "fvnet_conv.cu", "fvnet_ops.cu"],
-        "deps": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_ensemble.cu", "fv_kernels.cuh", "fv_physics.cuh",
+        "sources": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_ensemble.cu", "fvnet_conv.cu", "fvnet_ops.cu",
+                    "fv_selftest.cu"],
+        "deps": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_selftest.cu", "fv_ensemble.cu", "fv_kernels.cuh", "fv_physics.cuh",
                  "fvnet_conv.cu", "fvnet_ops.cu", "tc_sm100.cuh"],
         "flags": ["--fmad=false"],
         "headers": ["fv.h", "fvnet.h"],

@@ -30,11 +30,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return done != 0;
 }
 
-// Waits for the phase with an iteration limit; returns false (and sets *err) if it ran out.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, int* err) {
-    for (int it = 0; it < (1 << 22); ++it) {
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the phase with a time limit (try_wait may itself suspend the thread for a while, so the
+// bound is on elapsed time, not on the number of tries); returns false (and sets *err) if the limit
+// ran out.  The default limit, 1 s, is far above any legitimate wait in this library (microseconds).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, int* err,
+                                                  uint64_t limit_ns = 1000000000ull) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 0;; ++it) {
         if (mbar_try_wait(bar, phase)) return true;
-        if (it > 64) __nanosleep(64);
+        if ((it & 63u) == 63u) {
+            if (globaltimer_ns() - t0 > limit_ns) break;
+            __nanosleep(64);
+        }
     }
     if (err) atomicExch(err, 1);
     return false;
