@@ -314,22 +314,28 @@ __global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int npart
     dW[e] = s;
 }
 
-// db[co] = sum over pixels of dZ[p][co]: block partials, then a fixed-order sum.
-__global__ void bias_grad_partial_kernel(const __nv_bfloat16* __restrict__ dZ, long long npix, int cout_pad, int cout,
-                                         float* __restrict__ part) {
-    __shared__ float s[NT];
-    for (int co = 0; co < cout; ++co) {
-        float acc = 0.0f;
-        for (long long p = blockIdx.x * (long long)NT + threadIdx.x; p < npix; p += (long long)gridDim.x * NT)
-            acc += __bfloat162float(dZ[p * cout_pad + co]);
-        s[threadIdx.x] = acc;
-        __syncthreads();
-        for (int w = NT / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) part[blockIdx.x * cout + co] = s[0];
-        __syncthreads();
+// db[co] = sum over pixels of dZ[p][co]: block partials, then a fixed-order sum.  A thread reads whole
+// 16-byte chunks (8 channels of one pixel), consecutive threads consecutive chunks (coalesced), and
+// keeps 8 channel sums; the block then sums each channel over its threads in a fixed order.
+__global__ void __launch_bounds__(NT) bias_grad_partial_kernel(const uint4* __restrict__ dZ, long long npix, int cq,
+                                                               int cout, float* __restrict__ part) {
+    __shared__ float s[NT][9];  // padded: the column reads below hit distinct banks
+    const int t = threadIdx.x, q = t % cq, lp = t / cq, ppb = NT / cq;  // cq = cout_pad / 8 chunks per pixel
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (long long p = (long long)blockIdx.x * ppb + lp; p < npix; p += (long long)gridDim.x * ppb) {
+        const uint4 u = dZ[p * cq + q];
+        const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&u);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] += __bfloat162float(b[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s[t][j] = acc[j];
+    __syncthreads();
+    if (t < cq * 8) {
+        const int qq = t / 8, j = t % 8, c = 8 * qq + j;
+        float sum = 0.0f;
+        for (int k = qq; k < NT; k += cq) sum += s[k][j];
+        if (c < cout) part[blockIdx.x * cout + c] = sum;
     }
 }
 __global__ void bias_grad_reduce_kernel(const float* __restrict__ part, int nparts, int cout, float* __restrict__ db) {
@@ -468,7 +474,7 @@ int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int
     // parts actually used: CTAs whose row range is not empty
     const int used = (B * H + a.rows_per_cta - 1) / a.rows_per_cta;
     wgrad_reduce_kernel<<<(cout * cin * 9 + 255) / 256, 256, 0, st>>>(partial, used, cin_pad, cout_pad, cin, cout, dW);
-    bias_grad_partial_kernel<<<64, NT, 0, st>>>(static_cast<const __nv_bfloat16*>(dZ), (long long)B * H * W, cout_pad,
+    bias_grad_partial_kernel<<<64, NT, 0, st>>>(static_cast<const uint4*>(dZ), (long long)B * H * W, cout_pad / 8,
                                                 cout, db_part);
     bias_grad_reduce_kernel<<<1, 64, 0, st>>>(db_part, 64, cout, db);
     const cudaError_t e = cudaGetLastError();
