@@ -223,13 +223,21 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
     const uint32_t ab = tc::smem_addr(As), bb = tc::smem_addr(Bs);
     uint32_t phase = 0;
     bool ok = true;
+    int prev_n = -1, prev_y = -2;
     for (int row = r0; row < r1 && ok; ++row) {
         const int n = row / H, y = row % H;
+        // input rows y-1, y, y+1 live in a 3-slot ring keyed by the unwrapped row index u in [-1, H]
+        // (slot (u + 3) % 3; row u holds image row (u + H) % H): the next row of the same image
+        // loads only u = y + 1 into the slot of u = y - 2
+        const bool cont = (n == prev_n && y == prev_y + 1);
+        prev_n = n;
+        prev_y = y;
         uint4* Xs4 = reinterpret_cast<uint4*>(Xs);
-        for (int e = tid; e < 3 * W * CC; e += NT) {
-            const int cc = e % CC, t = e / CC, x = t % W, ky = t / W;
-            const int yy = (y + ky - 1 + H) % H;
-            Xs4[e] = a.X[(size_t(n * H + yy) * W + x) * CC + cc];
+        for (int e = tid; e < (cont ? 1 : 3) * W * CC; e += NT) {
+            const int cc = e % CC, t = e / CC, x = t % W;
+            const int ky = cont ? 2 : t / W;
+            const int u = y + ky - 1, slot = (u + 3) % 3;
+            Xs4[(slot * W + x) * CC + cc] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
         }
         uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
         for (int e = tid; e < W * OC; e += NT) Ds4[e] = a.dZ[size_t(n * H + y) * W * OC + e];
@@ -249,10 +257,10 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
                 uint32_t src, dst;
                 if (q < na) {
                     const int kc = q / NA, rest = q - kc * NA, sh = rest / CC, cc = rest - sh * CC;
-                    const int ky = sh / 3, kx = sh - ky * 3;
+                    const int ky = sh / 3, kx = sh - ky * 3, slot = (y + ky - 1 + 3) % 3;
                     int xs = kc * 8 + r8 + kx - 1;
                     xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
-                    src = xsb + uint32_t(((ky * W + xs) * CIN + cc * 8) * 2);
+                    src = xsb + uint32_t(((slot * W + xs) * CIN + cc * 8) * 2);
                     dst = ab + uint32_t((kc * MROWS + sh * CIN + cc * 8 + r8) * 16);
                 } else {
                     const int qb = q - na, kc = qb / OC, oc = qb - kc * OC;
