@@ -68,8 +68,11 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
     return u;
 }
 
+// Staging planes ([kx][cc] copies of the TR + 2 rows) are NPIX + 2 chunks apart: the 32-byte pad puts
+// the four channel chunks of one pixel, stored by neighbouring threads, in different bank groups.
+__host__ __device__ constexpr int conv_plane(int W) { return (256 / W + 2) * W + 2; }
 __host__ __device__ constexpr size_t conv_smem_bytes(int cin, int cout, int W) {
-    return size_t(3) * (cin / 8) * ((256 / W + 2) * W) * 16 + size_t(9) * (cin / 8) * cout * 16 + 64;
+    return size_t(3) * (cin / 8) * conv_plane(W) * 16 + size_t(9) * (cin / 8) * cout * 16 + 64;
 }
 
 template <int CIN, int COUT, int MODE>
@@ -77,9 +80,9 @@ __global__ void __launch_bounds__(NT) conv3x3_kernel(ConvArgs a) {
     constexpr int CC = CIN / 8;
     extern __shared__ __align__(1024) unsigned char smem[];
     const int W = a.W, H = a.H;
-    const int TR = 256 / W, NPIX = (TR + 2) * W;
-    uint4* Xc = reinterpret_cast<uint4*>(smem);                  // [3][CC][NPIX]
-    uint4* Wt = Xc + size_t(3) * CC * NPIX;                      // [9][CC][COUT]
+    const int TR = 256 / W, PS = conv_plane(W);
+    uint4* Xc = reinterpret_cast<uint4*>(smem);                  // [3][CC][PS] (NPIX used + pad)
+    uint4* Wt = Xc + size_t(3) * CC * PS;                        // [9][CC][COUT]
     uint64_t* bar = reinterpret_cast<uint64_t*>(Wt + 9 * CC * COUT);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(NT) conv3x3_kernel(ConvArgs a) {
 #pragma unroll
         for (int kx = 0; kx < 3; ++kx) {
             const int xd = (x - kx + 1 + W) % W;
-            Xc[(size_t(kx) * CC + cc) * NPIX + r * W + xd] = v;
+            Xc[(size_t(kx) * CC + cc) * PS + r * W + xd] = v;
         }
     }
     for (int e = tid; e < 9 * CC * COUT; e += NT) Wt[e] = a.Wb[e];
@@ -112,12 +115,12 @@ __global__ void __launch_bounds__(NT) conv3x3_kernel(ConvArgs a) {
     if (tid == 0) {
         constexpr uint32_t idesc = tc::idesc_bf16_f32(128, COUT);
         const uint32_t xb = tc::smem_addr(Xc), wb = tc::smem_addr(Wt);
-        const uint32_t lbo_a = uint32_t(NPIX) * 16, lbo_b = COUT * 16;
+        const uint32_t lbo_a = uint32_t(PS) * 16, lbo_b = COUT * 16;
         for (int mt = 0; mt < 2; ++mt)
             for (int sh = 0; sh < 9; ++sh) {
                 const int ky = sh / 3, kx = sh % 3;
                 for (int s = 0; s < CIN / 16; ++s) {
-                    const uint32_t aa = xb + ((kx * CC + 2 * s) * NPIX + mt * 128 + ky * W) * 16;
+                    const uint32_t aa = xb + ((kx * CC + 2 * s) * PS + mt * 128 + ky * W) * 16;
                     const uint32_t ba = wb + (sh * CC + 2 * s) * COUT * 16;
                     tc::mma_bf16(tmem + mt * COUT, tc::smem_desc(aa, lbo_a, 128), tc::smem_desc(ba, lbo_b, 128), idesc,
                                  (sh | s) != 0);
@@ -188,9 +191,11 @@ struct WgradArgs {
 };
 
 __host__ __device__ constexpr int wgrad_mrows(int cin) { return ((9 * cin + 127) / 128) * 128; }
+// Staged input / output-gradient rows keep 8 extra channels per pixel (16 bytes): the 8 pixel rows an
+// ldmatrix reads are then 80 (or 48) bytes apart instead of 64 (or 32) and fall in distinct bank groups.
 __host__ __device__ constexpr size_t wgrad_smem_bytes(int cin, int cout, int W) {
-    return size_t(W / 8) * wgrad_mrows(cin) * 16 + size_t(W / 8) * cout * 16 + size_t(3) * W * cin * 2 +
-           size_t(W) * cout * 2 + 64;
+    return size_t(W / 8) * wgrad_mrows(cin) * 16 + size_t(W / 8) * cout * 16 + size_t(3) * W * (cin + 8) * 2 +
+           size_t(W) * (cout + 8) * 2 + 64;
 }
 
 template <int CIN, int COUT>
@@ -201,9 +206,10 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
     const int W = a.W, H = a.H, KC = W / 8;
     uint4* As = reinterpret_cast<uint4*>(smem);                 // [KC][MROWS]
     uint4* Bs = As + size_t(KC) * MROWS;                        // [KC][COUT]
-    __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(Bs + KC * COUT);  // [3][W][CIN]
-    __nv_bfloat16* Ds = Xs + 3 * W * CIN;                        // [W][COUT]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + W * COUT);
+    constexpr int XP = CIN + 8, DP = COUT + 8;                   // padded pixel strides (bf16 elements)
+    __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(Bs + KC * COUT);  // [3][W][XP]
+    __nv_bfloat16* Ds = Xs + 3 * W * XP;                         // [W][DP]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + W * DP);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int total = a.B * H;
@@ -237,10 +243,10 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
             const int cc = e % CC, t = e / CC, x = t % W;
             const int ky = cont ? 2 : t / W;
             const int u = y + ky - 1, slot = (u + 3) % 3;
-            Xs4[(slot * W + x) * CC + cc] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
+            Xs4[(slot * W + x) * (CC + 1) + cc] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
         }
         uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
-        for (int e = tid; e < W * OC; e += NT) Ds4[e] = a.dZ[size_t(n * H + y) * W * OC + e];
+        for (int e = tid; e < W * OC; e += NT) Ds4[(e / OC) * (OC + 1) + e % OC] = a.dZ[size_t(n * H + y) * W * OC + e];
         __syncthreads();
         // A[kc][m = shift*CIN + ci] = X[y+ky-1][kc*8 + i + kx - 1][ci], i = 0..7 (periodic), and
         // B[kc][co] = dZ[kc*8 + i][co]: 8x8 bf16 transposes, four per warp instruction pair.  Lane l
@@ -260,11 +266,11 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
                     const int ky = sh / 3, kx = sh - ky * 3, slot = (y + ky - 1 + 3) % 3;
                     int xs = kc * 8 + r8 + kx - 1;
                     xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
-                    src = xsb + uint32_t(((slot * W + xs) * CIN + cc * 8) * 2);
+                    src = xsb + uint32_t(((slot * W + xs) * XP + cc * 8) * 2);
                     dst = ab + uint32_t((kc * MROWS + sh * CIN + cc * 8 + r8) * 16);
                 } else {
                     const int qb = q - na, kc = qb / OC, oc = qb - kc * OC;
-                    src = dsb + uint32_t(((kc * 8 + r8) * COUT + oc * 8) * 2);
+                    src = dsb + uint32_t(((kc * 8 + r8) * DP + oc * 8) * 2);
                     dst = bb + uint32_t((kc * COUT + oc * 8 + r8) * 16);
                 }
                 uint32_t v0, v1, v2, v3;
