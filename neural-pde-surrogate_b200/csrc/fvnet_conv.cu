@@ -229,25 +229,43 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
     const uint32_t ab = tc::smem_addr(As), bb = tc::smem_addr(Bs);
     uint32_t phase = 0;
     bool ok = true;
-    int prev_n = -1, prev_y = -2;
-    for (int row = r0; row < r1 && ok; ++row) {
+    uint4* Xs4 = reinterpret_cast<uint4*>(Xs);
+    uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
+    // Input rows y-1, y, y+1 live in a 3-slot ring keyed by the unwrapped row index u in [-1, H] (slot
+    // (u + 3) % 3; row u holds image row (u + H) % H).  A row that continues the previous one in the
+    // same image needs one new input row (u = y + 1, into the slot of u = y - 2) and its output-
+    // gradient row: those are prefetched into registers while the previous row is transposed, and
+    // stored once its transposes are done.  Rows that start a range or an image load all three.
+    constexpr int PF = 4;  // prefetch chunks per thread: W * CC / NT and W * OC / NT are at most 4
+    auto stage_rows = [&](int row, bool all) {  // synchronous load of a row's data into the ring
         const int n = row / H, y = row % H;
-        // input rows y-1, y, y+1 live in a 3-slot ring keyed by the unwrapped row index u in [-1, H]
-        // (slot (u + 3) % 3; row u holds image row (u + H) % H): the next row of the same image
-        // loads only u = y + 1 into the slot of u = y - 2
-        const bool cont = (n == prev_n && y == prev_y + 1);
-        prev_n = n;
-        prev_y = y;
-        uint4* Xs4 = reinterpret_cast<uint4*>(Xs);
-        for (int e = tid; e < (cont ? 1 : 3) * W * CC; e += NT) {
+        for (int e = tid; e < (all ? 3 : 1) * W * CC; e += NT) {
             const int cc = e % CC, t = e / CC, x = t % W;
-            const int ky = cont ? 2 : t / W;
+            const int ky = all ? t / W : 2;
             const int u = y + ky - 1, slot = (u + 3) % 3;
             Xs4[(slot * W + x) * (CC + 1) + cc] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
         }
-        uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
         for (int e = tid; e < W * OC; e += NT) Ds4[(e / OC) * (OC + 1) + e % OC] = a.dZ[size_t(n * H + y) * W * OC + e];
-        __syncthreads();
+    };
+    if (r0 < r1) stage_rows(r0, true);
+    __syncthreads();
+    for (int row = r0; row < r1 && ok; ++row) {
+        const int n = row / H, y = row % H;
+        const int nrow = row + 1;
+        const bool has_next = nrow < r1, next_cont = has_next && (nrow % H) != 0;
+        uint4 xpre[PF], dpre[PF];
+        if (next_cont) {  // issue the next row's loads now; they land during the transposes
+            const int yn = nrow % H, u = yn + 1;
+#pragma unroll
+            for (int k = 0; k < PF; ++k) {
+                const int e = tid + k * NT;
+                if (e < W * CC) {
+                    const int cc = e % CC, x = e / CC;
+                    xpre[k] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
+                }
+                if (e < W * OC) dpre[k] = a.dZ[size_t(n * H + yn) * W * OC + e];
+            }
+        }
         // A[kc][m = shift*CIN + ci] = X[y+ky-1][kc*8 + i + kx - 1][ci], i = 0..7 (periodic), and
         // B[kc][co] = dZ[kc*8 + i][co]: 8x8 bf16 transposes, four per warp instruction pair.  Lane l
         // names row l%8 of matrix l/8: ldmatrix.trans reads 8 pixel rows (16 bytes = 8 channels each)
@@ -280,7 +298,7 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
         }
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
+        __syncthreads();  // transposes done: A/B complete, and the ring slot of u = y - 1 is free
         tc::fence_after_sync();
         if (tid == 0) {
             for (int mt = 0; mt < MT; ++mt)
@@ -292,9 +310,22 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
                 }
             tc::mma_commit(bar);
         }
-        ok = tc::mbar_wait_bounded(bar, phase, a.err);
+        // the next row's data into the ring (the MMAs read only A and B)
+        if (next_cont) {
+            const int slot = (nrow % H + 1 + 3) % 3;
+#pragma unroll
+            for (int k = 0; k < PF; ++k) {
+                const int e = tid + k * NT;
+                if (e < W * CC) Xs4[(slot * W + e / CC) * (CC + 1) + e % CC] = xpre[k];
+                if (e < W * OC) Ds4[(e / OC) * (OC + 1) + e % OC] = dpre[k];
+            }
+        } else if (has_next) {
+            stage_rows(nrow, true);
+        }
+        ok = tc::mbar_wait_bounded(bar, phase, a.err);  // A and B are rewritten by the next row
         phase ^= 1;
         tc::fence_after_sync();
+        __syncthreads();  // the next row's data is visible
     }
     if (ok && r0 < r1) {
         for (int mt = 0; mt < MT; ++mt) {
