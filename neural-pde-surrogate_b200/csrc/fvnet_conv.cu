@@ -94,7 +94,9 @@ __global__ void __launch_bounds__(NT) conv3x3_kernel(ConvArgs a) {
         tc::mbar_init(bar, 1);
         tc::fence_mbar_init();
     }
-    // stage three x-shifted copies of rows y0-1 .. y0+TR (periodic in x and y)
+    // stage three x-shifted copies of rows y0-1 .. y0+TR (periodic in x and y); unrolled so that
+    // several global loads are in flight before their stores
+#pragma unroll 4
     for (int e = tid; e < (TR + 2) * W * CC; e += NT) {
         const int cc = e % CC, t = e / CC, x = t % W, r = t / W;
         const int y = (y0 - 1 + r + H) % H;
@@ -274,26 +276,37 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
         {
             const int r8 = lane & 7, mq = lane >> 3;
             constexpr int NA = 9 * CC;  // matrices per kc for A
-            const int na = KC * NA, nb = KC * OC;
+            constexpr int NW = NT / 32, ILP = 4;
+            const int na = KC * NA, nops = (na + KC * OC) / 4;  // x4 operations (4 matrices each)
             const uint32_t xsb = tc::smem_addr(Xs), dsb = tc::smem_addr(Ds);
-            for (int q0 = warp * 4; q0 < na + nb; q0 += 4 * (NT / 32)) {
-                const int q = q0 + mq;
-                uint32_t src, dst;
-                if (q < na) {
-                    const int kc = q / NA, rest = q - kc * NA, sh = rest / CC, cc = rest - sh * CC;
-                    const int ky = sh / 3, kx = sh - ky * 3, slot = (y + ky - 1 + 3) % 3;
-                    int xs = kc * 8 + r8 + kx - 1;
-                    xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
-                    src = xsb + uint32_t(((slot * W + xs) * XP + cc * 8) * 2);
-                    dst = ab + uint32_t((kc * MROWS + sh * CIN + cc * 8 + r8) * 16);
-                } else {
-                    const int qb = q - na, kc = qb / OC, oc = qb - kc * OC;
-                    src = dsb + uint32_t(((kc * 8 + r8) * DP + oc * 8) * 2);
-                    dst = bb + uint32_t((kc * COUT + oc * 8 + r8) * 16);
+            // warp w takes operations w, w + NW, ...; ILP of them at a time: all loads, then all stores
+            for (int k0 = warp; k0 < nops; k0 += ILP * NW) {
+                uint32_t v[ILP][4], dst[ILP];
+#pragma unroll
+                for (int j = 0; j < ILP; ++j) {
+                    const int k = k0 + j * NW;  // warp-uniform
+                    if (k >= nops) break;
+                    const int q = 4 * k + mq;
+                    uint32_t src;
+                    if (q < na) {
+                        const int kc = q / NA, rest = q - kc * NA, sh = rest / CC, cc = rest - sh * CC;
+                        const int ky = sh / 3, kx = sh - ky * 3, slot = (y + ky - 1 + 3) % 3;
+                        int xs = kc * 8 + r8 + kx - 1;
+                        xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
+                        src = xsb + uint32_t(((slot * W + xs) * XP + cc * 8) * 2);
+                        dst[j] = ab + uint32_t((kc * MROWS + sh * CIN + cc * 8 + r8) * 16);
+                    } else {
+                        const int qb = q - na, kc = qb / OC, oc = qb - kc * OC;
+                        src = dsb + uint32_t(((kc * 8 + r8) * DP + oc * 8) * 2);
+                        dst[j] = bb + uint32_t((kc * COUT + oc * 8 + r8) * 16);
+                    }
+                    tc::ldsm_x4_trans(src, v[j][0], v[j][1], v[j][2], v[j][3]);
                 }
-                uint32_t v0, v1, v2, v3;
-                tc::ldsm_x4_trans(src, v0, v1, v2, v3);
-                tc::stsm_x4(dst, v0, v1, v2, v3);
+#pragma unroll
+                for (int j = 0; j < ILP; ++j) {
+                    if (k0 + j * NW >= nops) break;
+                    tc::stsm_x4(dst[j], v[j][0], v[j][1], v[j][2], v[j][3]);
+                }
             }
         }
         tc::fence_proxy_async_smem();
