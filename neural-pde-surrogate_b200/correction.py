@@ -201,6 +201,19 @@ class CoarseSolver:
         return steps, status
 
 
+def load_checkpoint(path, B, H, W, gain=None, device="cuda"):
+    """A trained correction for B grids of H x W: (net, stats, dscale) ready for hybrid_step.
+    dscale includes the correction gain -- the checkpoint's evaluated setting (its `gain` entry,
+    1 if absent) unless `gain` is given."""
+    import torch
+    z = np.load(path)
+    g = float(z["gain"]) if gain is None and "gain" in z.files else (1.0 if gain is None else float(gain))
+    net = CorrectionNet(B, H, W, device=device, params=z["params"])
+    stats = torch.from_numpy(z["stats"]).to(device)
+    dscale = torch.from_numpy(z["dscale"]).to(device) * g
+    return net, stats, dscale
+
+
 def hybrid_step(net, coarse, U, dt_frame, stats, dscale, Uc, Unext, fallback, mode="scale"):
     """One hybrid step: Uc = coarse(U, dt_frame); Unext = Uc + projected correction under the
     positivity rule `mode` ('strict': fall back to the plain coarse step; 'scale': largest physical

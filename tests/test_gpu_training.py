@@ -60,7 +60,14 @@ def test_shipped_model_beats_the_plain_coarse_solver_in_rollouts():
     model = Path(tc.__file__).parent / "checkpoints" / "correction_64.npz"
     items = [("riemann", 200000 + k) for k in range(3)] + [("blast", 200000 + k) for k in range(3)]
     truth, first = pa.truth_frames(items, 512, 64, 10, [64], log=print)
-    hyb = pa.run_hybrid(str(model), first[64], 64, 10, truth, "scale", 0.75)
+    z = np.load(model)
+    assert float(z["gain"]) == 0.75  # the setting the checkpoint was evaluated with
+    import torch
+    corr = importlib.import_module("neural-pde-surrogate_b200.correction")
+    _, stats, dscale = corr.load_checkpoint(str(model), 2, 64, 64)
+    assert torch.equal(dscale.cpu(), torch.from_numpy(z["dscale"]) * 0.75)
+    assert torch.equal(stats.cpu(), torch.from_numpy(z["stats"]))
+    hyb = pa.run_hybrid(str(model), first[64], 64, 10, truth, "scale", float(z["gain"]))
     plain = pa.run_plain(first[64], 64, 64, 10, truth)
     print(hyb["L1_per_frame"], plain["L1_per_frame"])
     assert all(h < p for h, p in zip(hyb["L1_per_frame"], plain["L1_per_frame"]))
