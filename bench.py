@@ -146,7 +146,7 @@ def run_ours(args):
     dev_U = [torch.from_numpy(ic.to_conserved(*x)).to(f"cuda:{local}") for x in ics]
     dev_out = {m: torch.empty((NOUT + 1, 4, m, m), dtype=torch.float32, device=f"cuda:{local}") for m in SAVE}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")  # > L2 (126 MB)
-    # pinned host inputs/outputs for `e2e`
+    # pinned host inputs for `e2e`; frames come back into pageable numpy arrays
     host_prim = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in x] for x in ics]
     torch.cuda.synchronize()
 
