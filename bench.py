@@ -123,6 +123,14 @@ def make_ics(ic, n, count, seed0):
     return out
 
 
+def bench_config(n, world):
+    """The workload both arms report: the same keys and values for ours and the reference."""
+    return {"workload": f"blast+bubble {n}^2 FP64 periodic, t=0.2, 20 frames -> 128^2/64^2 f32, "
+                        f"4 flux x limiter combos per step", "grid": n, "frames": NOUT,
+            "combos": [f"{a}+{b}" for a, b in COMBOS], "parallelism": f"replicas x{world}",
+            "l2": "GPU arm: 256 MB buffer written before every step (state 8.4 MB is L2-resident within a step)"}
+
+
 def run_ours(args):
     import torch
     rank, world, local = env_rank()
@@ -234,10 +242,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded blast + bubble initial conditions)",
-        "config": {"workload": f"blast+bubble {n}^2 FP64 periodic, t=0.2, 20 frames -> 128^2/64^2 f32, "
-                               f"4 flux x limiter combos per step", "grid": n, "frames": NOUT,
-                   "combos": [f"{a}+{b}" for a, b in COMBOS], "parallelism": f"replicas x{world}",
-                   "l2": "256 MB buffer written before every step (state 8.4 MB is L2-resident within a step)"},
+        "config": bench_config(n, world),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": f"stage_kernel<stage {stage}>", "achieved": achieved, "peak": peak,
@@ -329,8 +334,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded blast + bubble initial conditions)",
-        "config": {"workload": f"blast+bubble {n}^2 FP64 periodic, t=0.2, 20 frames -> 128^2/64^2 f32, "
-                               f"4 flux x limiter combos per step", "grid": n},
+        "config": bench_config(n, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
