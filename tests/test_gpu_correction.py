@@ -246,3 +246,22 @@ def test_adamw_matches_optax_semantics():
         p = p - lr * upd
         assert abs(net.norm.item() - norm) / norm < 1e-6
     assert np.abs(net.params.cpu().numpy() - p).max() < 1e-5
+
+
+def test_network_is_translation_equivariant():
+    """Periodic convolutions commute with periodic shifts: tests/test_models.py:46-50 checks
+    roll(model(x)) == model(roll(x)) to 1e-5 for a (7, -13) shift. Every output pixel here accumulates its
+    taps and channels in the same order wherever it sits, so the rolled output is equal bit for bit."""
+    ic = importlib.import_module("neural-pde-surrogate_b200.ic")
+    B, n = 2, 64
+    rng = np.random.default_rng(11)
+    net = corr.CorrectionNet(B, n, n, params=rng.normal(0, 0.1, corr.param_count()).astype(np.float32))
+    U = torch.stack([torch.from_numpy(ic.to_conserved(*ic.sample("blast", k, n)[:4])) for k in range(B)]).cuda()
+    stats = torch.tensor([1.0, 0.0, 0.0, 2.5, 1.0, 1.0, 1.0, 0.3], dtype=torch.float64, device="cuda")
+    out = net.forward(U, stats).clone()
+    assert out.abs().max() > 0
+    for shift in [(7, -13), (5, 0), (0, 9), (13, 50)]:
+        rolled = net.forward(torch.roll(U, shift, dims=(1, 2)).contiguous(), stats).clone()
+        torch.cuda.synchronize()
+        net.check_device_error()
+        assert torch.equal(rolled, torch.roll(out, shift, dims=(1, 2))), shift
