@@ -1,6 +1,6 @@
 """Host-side logic of the learned part, on the CPU: the shipped checkpoint's format, the Pareto
-evaluation's helpers (held-out set, block average, L1 density error, drift, per-family means) and the
-trainer's normalisation statistics."""
+evaluation's helpers (held-out set, block average, L1 density error, drift, per-family means), the
+trainer's normalisation statistics and the structure of its pushforward step."""
 import importlib
 from pathlib import Path
 
@@ -63,3 +63,86 @@ def test_training_statistics():
     assert torch.equal(w[..., 0], U[0, 0, ..., 0]) and torch.equal(w[..., 2], U[0, 0, ..., 0])
     assert torch.equal(w[..., 3], U[0, 0, ..., 3])
     assert abs(corr.cosine_lr(0, 100, 1e-3, 10)) < 1e-12 and abs(corr.cosine_lr(100, 100, 1e-3, 10) - 1e-5) < 1e-15
+
+
+class _FakeNet:
+    def __init__(self, log):
+        self.log = log
+
+    def loss_grad(self, Un, y, Uc, stats, dscale, theta, loss_part):
+        self.log.append(("loss_grad", Un.clone(), y.clone(), None if theta is None else theta.clone()))
+        loss_part.fill_(2.0)
+
+    def backward(self):
+        self.log.append(("backward",))
+
+    def adamw(self, lr):
+        self.log.append(("adamw", lr))
+
+
+class _FakeCorr:
+    """hybrid_step stand-in: the next state is the input + 1; per-call coarse statuses from a list."""
+
+    def __init__(self, log, statuses):
+        self.log, self.statuses = log, list(statuses)
+
+    def hybrid_step(self, net, coarse, U, dt, stats, dscale, Uc, Un, fb, mode="scale"):
+        self.log.append(("hybrid", U.clone(), mode))
+        Un.copy_(U + 1.0)
+        return 1, self.statuses.pop(0)
+
+
+def _cpu_trainer(B, unroll, statuses):
+    tr = object.__new__(tc.Trainer)  # no CUDA buffers: every array of the step is a CPU tensor here
+    log = []
+    shape = (B, 2, 2, 4)
+    x0 = torch.arange(B * 16, dtype=torch.float64).reshape(shape)
+    y0 = -x0
+    tr.torch, tr.corr, tr.net, tr.coarse = torch, _FakeCorr(log, statuses), _FakeNet(log), None
+    tr.B, tr.unroll, tr.mode, tr.noise, tr.coarse_failures = B, unroll, "scale", 0.0, 0
+    tr.stats, tr.dscale = torch.ones(8, dtype=torch.float64), torch.ones(4, dtype=torch.float64)
+    tr.x, tr.Uc, tr.Un = (torch.empty(shape, dtype=torch.float64) for _ in range(3))
+    tr.fb = torch.zeros(B, dtype=torch.int32)
+    tr.loss_part = torch.zeros(B, dtype=torch.float64)
+    tr.ok = torch.ones(B, dtype=torch.float64)
+    tr._pairs = lambda U, k: (x0, y0)
+    tr.train_U = None
+    return tr, log, x0, y0
+
+
+def test_pushforward_step_trains_only_the_last_step():
+    """train.py:107-111's pushforward: unroll-1 self-fed hybrid steps give the trained step its input,
+    and one backward runs through that last step alone. Its gradient is therefore the gradient of a
+    one-step loss on a fixed input (tests/test_train.py:35-57 checks this equality in the reference),
+    not backpropagation through the chain, which would need a backward pass per unrolled step."""
+    B, unroll = 3, 4
+    ok = np.zeros(B, np.int32)
+    tr, log, x0, y0 = _cpu_trainer(B, unroll, [ok] * unroll)
+    loss = tr.step(1e-3)
+    hyb = [e for e in log if e[0] == "hybrid"]
+    assert [e[2] for e in hyb] == ["scale"] * (unroll - 1) + ["keep"]  # self-fed rule, then the full correction
+    for k, e in enumerate(hyb):
+        assert torch.equal(e[1], x0 + k)  # each step starts from the previous step's output
+    assert [e[0] for e in log[unroll:]] == ["loss_grad", "backward", "adamw"]  # after the whole unroll, once
+    _, Un, y, theta = log[unroll]
+    assert torch.equal(Un, x0 + unroll) and torch.equal(y, y0) and theta is None
+    assert float(loss) == 2.0 * B / (B * 16)
+    assert tr.coarse_failures == 0
+
+
+def test_one_step_training_is_the_unroll_one_case():
+    """With k = 1 the pushforward loss is the one-step loss (tests/test_train.py:37-39)."""
+    tr, log, x0, _ = _cpu_trainer(2, 4, [np.zeros(2, np.int32)])
+    tr.step(1e-3, unroll=1)
+    assert [e[0] for e in log] == ["hybrid", "loss_grad", "backward", "adamw"]
+    assert log[0][2] == "keep" and torch.equal(log[0][1], x0)
+
+
+def test_a_sample_whose_coarse_solve_stopped_gets_no_gradient():
+    B, unroll = 4, 3
+    st = [np.array([0, 0, 0, 0]), np.array([0, 3, 0, 0]), np.array([0, 0, 0, 3])]  # sample 1 self-fed, 3 trained
+    tr, log, _, _ = _cpu_trainer(B, unroll, st)
+    tr.step(1e-3)
+    theta = [e for e in log if e[0] == "loss_grad"][0][3]
+    assert theta.tolist() == [1.0, 0.0, 1.0, 0.0]
+    assert tr.coarse_failures == 2
