@@ -18,6 +18,10 @@ the rest; HDF5 is not available to this build).  While copying, every trajectory
 positivity of rho and p and for conservation of mass and energy over its frames (relative drift
 < 1e-5).  Normalisation statistics come from the train split only: per-field mean and std of U, of
 log rho, and of one-frame increments, PACKED/stats_<n>.json.
+
+Step 3, loading (surrogate/data.py): PairDataset serves (frame t, frames t+1 .. t+horizon) pairs of a
+packed split, normalised by Normaliser with the train statistics, from host memory or memory-mapped;
+PairDataset.states() puts a whole split in HBM for train_correction.py --packed.
 """
 import argparse
 import json
@@ -182,6 +186,95 @@ def load(packed, split, n, mmap=True):
     packed = Path(packed)
     U = np.load(packed / f"{split}_{n}_U.npy", mmap_mode="r" if mmap else None)
     return U, np.load(packed / f"{split}_{n}_t.npy"), json.loads((packed / f"{split}_{n}.json").read_text())
+
+
+# ---------------------------------------------------------------- loading for training (surrogate/data.py)
+
+
+class Normaliser:
+    """Per-variable affine map with the train split's statistics (PACKED/stats_<n>.json):
+    encode(U) = (U - mean) / std, decode(Z) = Z * std + mean, float32 statistics, the 4 variables on
+    axis `axis` (-3 for (..., 4, n, n)); the semantics of surrogate/data.py:19-40."""
+
+    def __init__(self, stats_path):
+        s = json.loads(Path(stats_path).read_text())
+        self.mean = np.asarray(s["mean"], np.float32)
+        self.std = np.asarray(s["std"], np.float32)
+        self.delta_std = np.asarray(s["delta_std"], np.float32)
+
+    def _on(self, v, ndim, axis):
+        return np.expand_dims(v, [d for d in range(ndim) if d != axis % ndim])
+
+    def encode(self, U, axis=-3):
+        return (U - self._on(self.mean, U.ndim, axis)) / self._on(self.std, U.ndim, axis)
+
+    def decode(self, Z, axis=-3):
+        return Z * self._on(self.std, Z.ndim, axis) + self._on(self.mean, Z.ndim, axis)
+
+
+class PairDataset:
+    """Every (trajectory, start frame) pair of one packed split at one resolution, with `horizon` target
+    frames: the interface of surrogate/data.py:43-101 (same names, pair order, normalisation and
+    errors) over the .npy packs written by pack().
+
+    x of pair (k, t) is frame t of trajectory k, y its frames t+1 .. t+horizon; a pair never runs past
+    its trajectory's last frame.  in_memory=True reads the split into host memory once; False keeps it
+    memory-mapped and reads only the frames each batch touches.  states() hands the whole split to the
+    GPU in the layout the coarse solver and the correction network use."""
+
+    def __init__(self, packed_dir, split, n, horizon=1, in_memory=True):
+        packed_dir = Path(packed_dir)
+        self.split, self.n, self.horizon, self.in_memory = split, n, horizon, in_memory
+        self.path = packed_dir / f"{split}_{n}_U.npy"
+        self.norm = Normaliser(packed_dir / f"stats_{n}.json")
+        meta = json.loads((packed_dir / f"{split}_{n}.json").read_text())
+        self.family = np.asarray(meta["family"])
+        self.index = np.asarray(meta["index"])
+        self.U = np.load(self.path, mmap_mode=None if in_memory else "r")
+        self.n_traj, self.n_frames = self.U.shape[:2]
+        if not 1 <= horizon < self.n_frames:
+            raise ValueError(f"horizon must be between 1 and {self.n_frames - 1}")
+        # trajectory-major: pair k * (F - horizon) + t is (k, t)
+        k, t = np.divmod(np.arange(self.n_traj * (self.n_frames - horizon)), self.n_frames - horizon)
+        self.pairs = np.stack([k, t], axis=1)
+
+    def __len__(self):
+        return len(self.pairs)
+
+    def _windows(self, pairs):
+        """Raw frames t .. t+horizon of each (k, t): (B, 1 + horizon, 4, n, n), one gather."""
+        pairs = np.asarray(pairs).reshape(-1, 2)
+        span = np.arange(self.horizon + 1)
+        return self.U[pairs[:, :1], pairs[:, 1:] + span]
+
+    def get(self, pairs):
+        """Normalised float32 (x (B, 4, n, n), y (B, horizon, 4, n, n)) of (trajectory, start) pairs."""
+        w = self.norm.encode(self._windows(pairs).astype(np.float32))
+        return w[:, 0], w[:, 1:]
+
+    def batches(self, batch_size, rng=None, shuffle=True, drop_last=True):
+        """One pass over the pairs (shuffled by `rng` when shuffle), batch_size pairs at a time."""
+        order = np.arange(len(self.pairs))
+        if shuffle:
+            (rng if rng is not None else np.random.default_rng()).shuffle(order)
+        end = len(order) - len(order) % batch_size if drop_last else len(order)
+        for s in range(0, end, batch_size):
+            yield self.get(self.pairs[order[s:s + batch_size]])
+
+    def trajectory(self, k, normalised=True):
+        """All frames of trajectory k, (F, 4, n, n) float32, normalised unless asked otherwise."""
+        U = np.asarray(self.U[k], np.float32)
+        return self.norm.encode(U) if normalised else U
+
+    def states(self, device="cuda"):
+        """The whole split as an (N, F, n, n, 4) float64 torch tensor on `device`: conserved states per
+        cell, channels last, unnormalised -- what the trainer samples its batches from on the device
+        (a 64^2 split of 512 trajectories x 41 frames is 2.7 GB in FP64)."""
+        import torch
+        out = torch.empty((self.n_traj, self.n_frames, self.n, self.n, 4), dtype=torch.float64, device=device)
+        for k in range(self.n_traj):  # one trajectory at a time: host memory stays one trajectory wide
+            out[k].copy_(torch.from_numpy(np.ascontiguousarray(self.U[k].transpose(0, 2, 3, 1))))
+        return out
 
 
 def main():

@@ -5,7 +5,8 @@
 
 Data: n_traj trajectories (half four-quadrant Riemann, half blast + bubble initial conditions,
 indices [index0, index0 + n_traj/2) of each family) solved by the FP64 GPU solver at fine^2 and
-block-averaged to coarse^2 every 0.005 in time (generate.trajectory).  Normalisation statistics are
+block-averaged to coarse^2 every 0.005 in time (generate.trajectory); or, with --packed DIR, the
+train and val splits that generate.py and dataset.py wrote to DIR.  Normalisation statistics are
 taken from these training frames only (data/pack.py:54-112 does the same).
 
 Model step (correction.hybrid_step): the coarse FP64 solver advances one frame interval, the CNN
@@ -205,8 +206,15 @@ def train(cfg, log=print):
     if out:
         out.mkdir(parents=True, exist_ok=True)
     t0 = time.time()
-    train_U = build_dataset(cfg["n_traj"], cfg["fine"], cfg["coarse"], index0=0, log=log)
-    val_U = build_dataset(cfg["n_val"], cfg["fine"], cfg["coarse"], index0=100000, log=log)
+    if cfg.get("packed"):  # the generate.py -> dataset.py pipeline's packs: train and val splits
+        dsm = importlib.import_module(f"{PKG}.dataset")
+        train_U = dsm.PairDataset(cfg["packed"], "train", cfg["coarse"]).states()
+        val_U = dsm.PairDataset(cfg["packed"], "val", cfg["coarse"]).states()
+        log(f"dataset: packed {cfg['packed']}: train {tuple(train_U.shape[:2])}, val {tuple(val_U.shape[:2])} "
+            f"(trajectories, frames) at {cfg['coarse']}^2")
+    else:
+        train_U = build_dataset(cfg["n_traj"], cfg["fine"], cfg["coarse"], index0=0, log=log)
+        val_U = build_dataset(cfg["n_val"], cfg["fine"], cfg["coarse"], index0=100000, log=log)
     tr = Trainer(train_U, val_U, cfg["batch"], cfg["unroll"], seed=cfg["seed"], log=log, init=cfg.get("init"))
     tr.noise = float(cfg.get("noise", 0.0))
     corr = tr.corr
@@ -262,6 +270,9 @@ def train(cfg, log=print):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--out", default="runs/correction")
+    ap.add_argument("--packed", default=None,
+                    help="train on this packed directory (dataset.py output: its train and val splits at "
+                         "--coarse) instead of solving --n-traj / --n-val trajectories at --fine")
     ap.add_argument("--n-traj", type=int, default=512)
     ap.add_argument("--n-val", type=int, default=32)
     ap.add_argument("--fine", type=int, default=512)

@@ -67,3 +67,81 @@ def test_pack_flags_nonpositive_density(tmp_path):
     _write_raw(raw, "riemann", 1, 4, bad_rho=True)
     assert not ds.pack(raw, out, sizes=(8,), log=lambda *a: None)
     assert not json.loads((out / "train_8.json").read_text())["checks_passed"]
+
+
+@pytest.fixture(scope="module")
+def packed(tmp_path_factory):
+    root = tmp_path_factory.mktemp("pairs")
+    raw, out = root / "raw", root / "packed"
+    for i in range(20):
+        _write_raw(raw, "riemann", i, 7)
+    for i in range(10):
+        _write_raw(raw, "blast", i, 6)
+    assert ds.pack(raw, out, sizes=(8,), log=lambda *a: None)
+    return out
+
+
+def test_pairs_cover_every_start_frame_and_line_up(packed):
+    """The checks of the reference's tests/test_data.py:21-28 on the packs written here."""
+    d = ds.PairDataset(packed, "train", 8, horizon=1)
+    F = d.n_frames
+    assert (d.n_traj, F) == (24, 6) and len(d) == d.n_traj * (F - 1)
+    assert d.pairs[:, 1].max() == F - 2 and d.pairs[:, 1].min() == 0
+    assert d.pairs[F - 1].tolist() == [1, 0]  # trajectory-major order
+    x0, y0 = d.get([(0, 2)])
+    x1, _ = d.get([(0, 3)])
+    assert np.array_equal(y0[0, 0], x1[0])  # the target of (k, t) is the input of (k, t + 1)
+    assert list(d.family[:2]) == ["blast", "blast"] and d.index[0] == 0
+
+
+def test_normalisation_uses_the_train_statistics(packed):
+    d = ds.PairDataset(packed, "train", 8)
+    raw = d.trajectory(3, normalised=False)
+    assert np.allclose(d.norm.decode(d.norm.encode(raw)), raw, rtol=1e-5, atol=1e-5)
+    z = np.concatenate([d.trajectory(k) for k in range(d.n_traj)])
+    assert np.abs(z.mean(axis=(0, 2, 3))).max() < 1e-4 and np.abs(z.std(axis=(0, 2, 3)) - 1).max() < 1e-3
+    st = json.loads((packed / "stats_8.json").read_text())
+    assert np.array_equal(d.norm.delta_std, np.asarray(st["delta_std"], np.float32))
+    # the variable axis can be any axis: channels-last states normalise the same way
+    cl = raw.transpose(0, 2, 3, 1)
+    assert np.allclose(d.norm.encode(cl, axis=-1).transpose(0, 3, 1, 2), d.norm.encode(raw), atol=1e-6)
+    # val and test are normalised with the train statistics, not their own
+    v = ds.PairDataset(packed, "val", 8)
+    assert np.array_equal(v.norm.mean, d.norm.mean) and np.array_equal(v.norm.std, d.norm.std)
+
+
+def test_batches_shapes_and_reproducibility(packed):
+    d = ds.PairDataset(packed, "train", 8)
+    x, y = next(d.batches(8, rng=np.random.default_rng(1)))
+    assert x.shape == (8, 4, 8, 8) and y.shape == (8, 1, 4, 8, 8)
+    assert x.dtype == np.float32 and y.dtype == np.float32
+    xa, _ = next(d.batches(8, rng=np.random.default_rng(1)))
+    assert np.array_equal(x, xa)
+    assert sum(1 for _ in d.batches(7, rng=np.random.default_rng(0))) == len(d) // 7
+    assert sum(len(b[0]) for b in d.batches(7, drop_last=False, shuffle=False)) == len(d)
+    xs, _ = next(d.batches(3, shuffle=False))
+    assert np.array_equal(xs, d.get(d.pairs[:3])[0])
+
+
+def test_multistep_targets_and_disk_mode(packed):
+    d3 = ds.PairDataset(packed, "train", 8, horizon=3)
+    x, y = d3.get([(2, 1)])
+    traj = d3.trajectory(2)
+    assert np.array_equal(y[0], traj[2:5]) and np.array_equal(x[0], traj[1])
+    assert d3.pairs[:, 1].max() == d3.n_frames - 4
+    mem = ds.PairDataset(packed, "train", 8, horizon=1)
+    disk = ds.PairDataset(packed, "train", 8, horizon=1, in_memory=False)
+    sel = mem.pairs[[0, 7, 50 % len(mem)]]
+    for a, b in zip(disk.get(sel), mem.get(sel)):
+        assert np.array_equal(a, b)
+    for h in (0, mem.n_frames):
+        with pytest.raises(ValueError, match="horizon must be between 1 and 5"):
+            ds.PairDataset(packed, "train", 8, horizon=h)
+
+
+def test_states_are_channels_last_fp64(packed):
+    d = ds.PairDataset(packed, "val", 8, in_memory=False)
+    S = d.states(device="cpu")
+    assert tuple(S.shape) == (d.n_traj, d.n_frames, 8, 8, 4) and str(S.dtype) == "torch.float64"
+    U, _, _ = ds.load(packed, "val", 8)
+    assert np.array_equal(S.numpy(), np.asarray(U, np.float64).transpose(0, 1, 3, 4, 2))
