@@ -14,7 +14,9 @@ it on its own GPU; only the per-rank counts are gathered at the end (gloo, no da
 Output per trajectory: DIR/<family>/<index:06d>.npz with `t` (frames,) and `U_<m>` (frames, 4, m, m)
 float32 conserved variables per save size, plus the run attributes the reference stores
 (trajectory.hpp:74-89) and provenance (generate.py:87-97).  The file appears atomically
-(os.replace), so an interrupted batch can simply be restarted: existing files are skipped.
+(os.replace), so an interrupted batch can simply be restarted: existing files are skipped.  A
+trajectory that stops at a non-physical state leaves DIR/<family>/<index:06d>.failed.txt with the
+solver's report instead, and the batch carries on.
 """
 import argparse
 import datetime
@@ -60,13 +62,23 @@ def trajectory(family, index, n, save, flux="hllc", limiter="vanleer", cfl=0.5, 
 
 
 def generate_one(family, index, n, save, out_dir, force=False, solver=None):
-    """One file; returns 'done' or 'skipped' (data/generate.py:60-105 without the subprocess)."""
+    """One file; returns 'done', 'skipped' (the file exists) or 'failed' (details in
+    <index>.failed.txt) -- data/generate.py:60-105 without the subprocess."""
     final = Path(out_dir) / family / f"{index:06d}.npz"
     if final.exists() and not force:
         return "skipped"
     final.parent.mkdir(parents=True, exist_ok=True)
+    failed = final.with_suffix(".failed.txt")
+    FVError = importlib.import_module("neural-pde-surrogate_b200").FVError
     t0 = time.time()
-    t, levels, steps, params = trajectory(family, index, n, save, solver=solver)
+    try:
+        t, levels, steps, params = trajectory(family, index, n, save, solver=solver)
+    except FVError as e:
+        # a non-physical state (or a rejected initial condition): logged beside the output, and the
+        # batch goes on with the next index (data/generate.py:79-84); a restart retries it
+        failed.write_text(f"{family} {index} at {n}x{n}, save {list(save)}: failed after "
+                          f"{time.time() - t0:.1f} s\n{e}\n")
+        return "failed"
     attrs = {"family": family, "index": index, "steps": steps, "solver_nx": n, "solver_ny": n, "gamma": 1.4, "cfl": 0.5,
              "scheme": "hllc", "limiter": "vanleer", "bc_x": "periodic", "bc_y": "periodic", "t_start": float(t[0]),
              "t_end": float(t[-1]), "frames": len(t), "variables": "rho, rho*u, rho*v, E",
@@ -77,6 +89,8 @@ def generate_one(family, index, n, save, out_dir, force=False, solver=None):
                  **{f"param_{k}": np.asarray(v) for k, v in params.items() if k not in ("family", "index")},
                  **{f"attr_{k}": np.asarray(v) for k, v in attrs.items()})
     os.replace(tmp.name, final)  # the file appears only once complete
+    if failed.exists():
+        failed.unlink()  # an earlier attempt's log
     return "done"
 
 
@@ -109,8 +123,8 @@ def main():
     status = shard.run_sharded(indices, lambda i: generate_one(a.family, i, a.n, save, a.out, a.force, solver),
                                costs=costs)
     if status is not None:
-        print(f"Finished in {time.time() - t0:.1f} s: {status.count('done')} done, {status.count('skipped')} skipped"
-              f" on {world} GPU(s)")
+        print(f"Finished in {time.time() - t0:.1f} s: {status.count('done')} done, {status.count('skipped')} skipped, "
+              f"{status.count('failed')} failed on {world} GPU(s)")
     if world > 1:
         dist.destroy_process_group()
 
