@@ -68,6 +68,19 @@ def profiled_traffic():
     return profiled("traffic_bytes_per_launch_stage2")
 
 
+def fp64_roofline(n, stage1_ms):
+    """What binds the stage kernels instead of HBM: FP64 flop rate of the HLLC + van Leer stage-1
+    kernel, from its executed flops per cell (ncu count, committed summary) and its live mean launch
+    time `stage1_ms`, against the measured FP64 peak.  None without the summary's figures."""
+    flops, peak = profiled("fp64_flops_per_cell_stage1"), profiled("fp64_peak_tflops")
+    if flops is None or peak is None or not stage1_ms > 0:
+        return None
+    achieved = flops * n * n / (stage1_ms / 1e3) / 1e12
+    return {"kernel": "stage_kernel<stage 1> hllc+vanleer", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "flops_per_cell": flops, "peak_source": "measured (fv_fp64_peak, DFMA loop)",
+            "pipe_active_ncu": profiled("fp64_pipe_active_stage1")}
+
+
 class Clocks:
     """Samples nvidia-smi during the timed region."""
 
@@ -250,7 +263,8 @@ def run_ours(args):
                      "peak_source": peak_kind, "algorithmic_bytes_per_cell": STAGE_BYTES[stage],
                      "mean_launch_ms": {"stage1": ms1, "stage2": ms2},
                      # what binds instead: the FP64 pipe (ncu share of active cycles, committed summary)
-                     "fp64_pipe_active_ncu": profiled("fp64_pipe_active_stage2")},
+                     "fp64_pipe_active_ncu": profiled("fp64_pipe_active_stage2"),
+                     "fp64": fp64_roofline(n, stage_ms[COMBOS.index(("hllc", "vanleer"))][0])},
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -76,3 +76,15 @@ def test_clock_summary_flags_slowdowns(tmp_path):
     c.path = str(tmp_path / "clocks.csv")
     Path(c.path).write_text("1200, 1965, 700.0, Active, Not Active, Active, Not Active\n")
     assert c.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+
+
+def test_fp64_roofline_of_the_stage_kernel(tmp_path, monkeypatch):
+    r = bench.fp64_roofline(512, 0.0238)  # a 23.8 us stage-1 launch at 512^2
+    assert r["unit"] == "TFLOP/s" and r["flops_per_cell"] == 542.0 and r["peak"] == 36.2
+    assert r["achieved"] == pytest.approx(542 * 512 * 512 / 23.8e-6 / 1e12)  # ~5.97 TFLOP/s
+    assert r["frac"] == pytest.approx(r["achieved"] / 36.2) and 0.1 < r["frac"] < 0.25
+    assert r["pipe_active_ncu"] == 0.407
+    assert bench.fp64_roofline(512, 0.0) is None  # no timed launches
+    monkeypatch.setattr(bench, "ROOT", tmp_path)  # no committed summary: no figure, no error
+    assert bench.fp64_roofline(512, 0.0238) is None
+    assert bench.profiled_traffic() is None
