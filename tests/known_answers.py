@@ -1,7 +1,8 @@
 """The reference's own known-answer checks, restated once and run against any implementation.
 
 Sources (GusGus2004/neural-pde-surrogate): solver/src/test_solver2d.cpp:35-108,
-test_riemann2d.cpp:17-47, test_grid2d.cpp:33-63, README.md:36-64 (validation numbers).
+test_riemann2d.cpp:17-47, test_grid2d.cpp:33-63, README.md:36-69 (validation numbers: Sod errors, Lax-Liu symmetry,
+Kelvin-Helmholtz growth rates).
 Each function takes a factory make(g, flux, limiter, cfl) returning an object with set_state /
 get_state / compute_dt / step (the interface shared by oracle.OracleSolver and the GPU Solver).
 """
@@ -93,3 +94,39 @@ def sod_l1(U, n):
     x = (np.arange(n) + 0.5) / n
     exact, _, _ = exact_riemann((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), x, 0.5, 0.2)
     return float(np.sum(np.abs(U[0, :, 0] - exact[:, 0])) * (1.0 / n))
+
+
+def kh_mode_amplitude(U, n):
+    """Amplitude of the seeded sin(4 pi x) mode of v near the two shear layers: the diagnostic of
+    McNally, Lyra & Passy (2012), eqs. 4-7, applied as experiments/kh_growth.py:17-27 applies it."""
+    x = ic.cell_centres(n)
+    X, Y = np.meshgrid(x, x)
+    v = U[..., 2] / U[..., 0]
+    w = np.exp(-4.0 * np.pi * np.where(Y < 0.5, np.abs(Y - 0.25), np.abs(0.75 - Y)))
+    s = np.sum(v * np.sin(4.0 * np.pi * X) * w) / np.sum(w)
+    c = np.sum(v * np.cos(4.0 * np.pi * X) * w) / np.sum(w)
+    return 2.0 * float(np.hypot(s, c))
+
+
+def kh_growth_rate(make, n, nout=20, t_end=2.0, window=(0.6, 1.2)):
+    """Exponential growth rate of the seeded KH mode (the driver's `kh` test, HLLC + van Leer):
+    frames at the driver's times t_end * k / nout (main2d.cpp:236-242), the slope of log amplitude
+    fitted over `window` (experiments/kh_growth.py:38-40)."""
+    g, _, U0 = ic.test_problem("kh", n)
+    s = make(g, "hllc", "vanleer", 0.5)
+    s.set_state(U0)
+    t, ts, amps = 0.0, [0.0], [kh_mode_amplitude(U0, n)]
+    for k in range(1, nout + 1):
+        t_next = 0.0 + ((t_end - 0.0) * k) / nout
+        if t_next > window[1] + 1e-12:
+            break
+        while t < t_next:
+            dt = s.compute_dt()
+            dt = (t_next - t) if (t_next - t) < dt else dt
+            s.step(dt)
+            t += dt
+        ts.append(t)
+        amps.append(kh_mode_amplitude(s.get_state(), n))
+    ts, amps = np.array(ts), np.array(amps)
+    sel = (ts >= window[0] - 1e-12) & (ts <= window[1] + 1e-12)
+    return float(np.polyfit(ts[sel], np.log(amps[sel]), 1)[0]), amps

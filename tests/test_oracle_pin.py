@@ -197,3 +197,14 @@ def test_exact_sod_star_state():
     from oracle.exact_riemann import star_state
     ps, us = star_state((1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
     assert round(ps, 5) == 0.30313 and round(us, 5) == 0.92745
+
+
+def test_kh_growth_rates_match_the_reference_validation():
+    """README.md:66-69 / experiments/results.md:98-102: the seeded KH mode decays at 16^2 and grows at
+    1.20, 2.41 and 2.71 at 32^2, 64^2 and 128^2 (HLLC + van Leer, fit over 0.6 <= t <= 1.2)."""
+    mk = lambda g, f, l, c: cpu_solver("oracle", g, f, l, c)
+    assert ka.kh_growth_rate(mk, 16)[0] < 0.0
+    for n, published in ((32, 1.20), (64, 2.41), (128, 2.71)):
+        rate, amps = ka.kh_growth_rate(mk, n)
+        assert abs(rate - published) < 0.01, (n, rate, published)
+        assert amps[0] == pytest.approx(0.01)  # the seeded amplitude, v = 0.01 sin(4 pi x)
