@@ -136,6 +136,18 @@ def make_ics(ic, n, count, seed0):
     return out
 
 
+def reduce_over_ranks(ms, cells, device):
+    """Whole-job figures of one timed region under torchrun: the slowest rank's time (MAX) and the
+    cell-updates of all ranks (SUM).  Every rank calls it at the same point."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([cells], device=device, dtype=torch.float64)
+    dist.all_reduce(c)
+    return float(t.item()), float(c.item())
+
+
 def bench_config(n, world):
     """The workload both arms report: the same keys and values for ours and the reference."""
     return {"workload": f"blast+bubble {n}^2 FP64 periodic, t=0.2, 20 frames -> 128^2/64^2 f32, "
@@ -220,13 +232,7 @@ def run_ours(args):
         ms = ev0.elapsed_time(ev1)
         launches = sum(solver_mod.launch_count(s) for s in solvers) - l0
         if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-            c = torch.tensor([cells], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(c)
-            cells = float(c.item())
+            ms, cells = reduce_over_ranks(ms, cells, f"cuda:{local}")
         return ms, cells, launches
 
     with Clocks(local) as clk:

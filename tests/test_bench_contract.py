@@ -88,3 +88,27 @@ def test_fp64_roofline_of_the_stage_kernel(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "ROOT", tmp_path)  # no committed summary: no figure, no error
     assert bench.fp64_roofline(512, 0.0238) is None
     assert bench.profiled_traffic() is None
+
+
+def _reduce_worker(rank, world, port, out_dir):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    import bench as b
+    ms, cells = b.reduce_over_ranks(10.0 + 5.0 * rank, 1000.0 * (rank + 1), "cpu")
+    (Path(out_dir) / f"r{rank}.json").write_text(json.dumps([ms, cells]))
+    dist.destroy_process_group()
+
+
+def test_timing_is_the_max_over_ranks_and_work_the_sum(tmp_path):
+    """The N > 1 reduction of bench.py's timed regions, as 2 gloo ranks on the CPU."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.start_processes(_reduce_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    for r in range(2):
+        assert json.loads((tmp_path / f"r{r}.json").read_text()) == [15.0, 3000.0]
