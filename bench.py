@@ -136,16 +136,16 @@ def make_ics(ic, n, count, seed0):
     return out
 
 
-def reduce_over_ranks(ms, cells, device):
-    """Whole-job figures of one timed region under torchrun: the slowest rank's time (MAX) and the
-    cell-updates of all ranks (SUM).  Every rank calls it at the same point."""
+def reduce_over_ranks(ms, cells, launches, device):
+    """Whole-job figures of one timed region under torchrun: the slowest rank's time (MAX), and the
+    cell-updates and kernel launches of all ranks (SUM).  Every rank calls it at the same point."""
     import torch
     import torch.distributed as dist
     t = torch.tensor([ms], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    c = torch.tensor([cells], device=device, dtype=torch.float64)
+    c = torch.tensor([cells, launches], device=device, dtype=torch.float64)
     dist.all_reduce(c)
-    return float(t.item()), float(c.item())
+    return float(t.item()), float(c[0].item()), int(c[1].item())
 
 
 def bench_config(n, world):
@@ -232,7 +232,7 @@ def run_ours(args):
         ms = ev0.elapsed_time(ev1)
         launches = sum(solver_mod.launch_count(s) for s in solvers) - l0
         if world > 1:
-            ms, cells = reduce_over_ranks(ms, cells, f"cuda:{local}")
+            ms, cells, launches = reduce_over_ranks(ms, cells, launches, f"cuda:{local}")
         return ms, cells, launches
 
     with Clocks(local) as clk:

@@ -97,13 +97,14 @@ def _reduce_worker(rank, world, port, out_dir):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
     import bench as b
-    ms, cells = b.reduce_over_ranks(10.0 + 5.0 * rank, 1000.0 * (rank + 1), "cpu")
-    (Path(out_dir) / f"r{rank}.json").write_text(json.dumps([ms, cells]))
+    out = b.reduce_over_ranks(10.0 + 5.0 * rank, 1000.0 * (rank + 1), 7 + rank, "cpu")
+    (Path(out_dir) / f"r{rank}.json").write_text(json.dumps(list(out)))
     dist.destroy_process_group()
 
 
 def test_timing_is_the_max_over_ranks_and_work_the_sum(tmp_path):
-    """The N > 1 reduction of bench.py's timed regions, as 2 gloo ranks on the CPU."""
+    """The N > 1 reduction of bench.py's timed regions (time: max; work and launches: sum), as 2 gloo
+    ranks on the CPU."""
     import socket
     import torch.multiprocessing as mp
     with socket.socket() as s:
@@ -111,4 +112,4 @@ def test_timing_is_the_max_over_ranks_and_work_the_sum(tmp_path):
         port = s.getsockname()[1]
     mp.start_processes(_reduce_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
     for r in range(2):
-        assert json.loads((tmp_path / f"r{r}.json").read_text()) == [15.0, 3000.0]
+        assert json.loads((tmp_path / f"r{r}.json").read_text()) == [15.0, 3000.0, 15]
