@@ -81,11 +81,18 @@ def fp64_roofline(n, stage1_ms):
             "pipe_active_ncu": profiled("fp64_pipe_active_stage1")}
 
 
+def smi_id(local):
+    """nvidia-smi's id of CUDA device `local`: nvidia-smi ignores CUDA_VISIBLE_DEVICES, so a masked
+    process maps its ordinal through the mask (an index or a UUID, both accepted by --id)."""
+    ids = [x.strip() for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+    return ids[local] if local < len(ids) else str(local)
+
+
 class Clocks:
     """Samples nvidia-smi during the timed region."""
 
-    def __init__(self, index):
-        self.index = index
+    def __init__(self, local):
+        self.index = smi_id(local)
         self.proc = None
         self.path = None
 

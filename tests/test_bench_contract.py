@@ -113,3 +113,13 @@ def test_timing_is_the_max_over_ranks_and_work_the_sum(tmp_path):
     mp.start_processes(_reduce_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
     for r in range(2):
         assert json.loads((tmp_path / f"r{r}.json").read_text()) == [15.0, 3000.0, 15]
+
+
+def test_clock_sampling_follows_the_device_mask(monkeypatch):
+    monkeypatch.delenv("CUDA_VISIBLE_DEVICES", raising=False)
+    assert bench.smi_id(0) == "0" and bench.smi_id(3) == "3"
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "5,2")
+    assert bench.smi_id(0) == "5" and bench.smi_id(1) == "2"
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "GPU-8f1e, GPU-77aa")
+    assert bench.smi_id(1) == "GPU-77aa"
+    assert bench.Clocks(0).index == "GPU-8f1e"
