@@ -199,6 +199,14 @@ class Trainer:
         return h / batches, c / batches
 
 
+def update_lr(step, cfg):
+    """Learning rate of the step-th update (1-based).  optax evaluates its schedule at the number of
+    updates already applied, so update k uses schedule(k - 1): the first update has the warm-up's
+    initial value 0 (train.py:209-211, optax.warmup_cosine_decay_schedule)."""
+    corr = importlib.import_module(f"{PKG}.correction")
+    return corr.cosine_lr(step - 1, cfg["steps"], cfg["lr"], min(cfg["warmup"], cfg["steps"] // 2))
+
+
 def train(cfg, log=print):
     """cfg: dict (see main()).  Returns (trainer, history rows)."""
     import torch
@@ -233,7 +241,7 @@ def train(cfg, log=print):
     t_train = time.time()
     onestep_until = int(cfg.get("onestep_frac", 0.0) * cfg["steps"])
     for step in range(1, cfg["steps"] + 1):
-        lr = corr.cosine_lr(step, cfg["steps"], cfg["lr"], min(cfg["warmup"], cfg["steps"] // 2))
+        lr = update_lr(step, cfg)
         # curriculum: one-step training first, so that the self-fed steps of the pushforward start from
         # a model whose own rollouts are close to the data (the reference fine-tunes with --init); then
         # pushforward steps alternate with one-step steps, which keep the one-step map anchored

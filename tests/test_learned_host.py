@@ -5,6 +5,7 @@ import importlib
 from pathlib import Path
 
 import numpy as np
+import pytest
 import torch
 
 corr = importlib.import_module("neural-pde-surrogate_b200.correction")
@@ -146,3 +147,15 @@ def test_a_sample_whose_coarse_solve_stopped_gets_no_gradient():
     theta = [e for e in log if e[0] == "loss_grad"][0][3]
     assert theta.tolist() == [1.0, 0.0, 1.0, 0.0]
     assert tr.coarse_failures == 2
+
+
+def test_update_k_uses_optax_schedule_count_k_minus_one():
+    cfg = {"steps": 1000, "lr": 1e-3, "warmup": 500}
+    assert tc.update_lr(1, cfg) == 0.0  # optax: schedule(0) = init_value
+    warm = min(500, 1000 // 2)
+    assert tc.update_lr(warm + 1, cfg) == pytest.approx(1e-3)  # the peak, at count = warmup
+    assert tc.update_lr(2, cfg) == pytest.approx(1e-3 / warm)
+    assert tc.update_lr(1000, cfg) == pytest.approx(corr.cosine_lr(999, 1000, 1e-3, warm))
+    assert tc.update_lr(1000, cfg) > 1e-5  # the end value is reached only at count = steps
+    cfg_short = {"steps": 100, "lr": 2e-3, "warmup": 500}  # warm-up capped at half the steps
+    assert tc.update_lr(51, cfg_short) == pytest.approx(2e-3)
