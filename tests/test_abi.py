@@ -67,3 +67,39 @@ def test_no_cpu_fallback(fvpkg):
     g = fvpkg.make_grid(8, 8, 0, 1, 0, 1, "periodic", "periodic")
     with pytest.raises(fvpkg.FVError, match="no CUDA device"):
         fvpkg.Solver(g, "hllc", "vanleer")
+
+
+def test_ensemble_and_network_argument_validation_without_gpu(fvpkg):
+    """Bad arguments are rejected before any CUDA call; valid ones on a machine without a GPU give
+    FV_ERR_CUDA, never a crash or a CPU computation."""
+    import torch
+    L = fvpkg.lib()
+    e = C.c_void_p()
+    ints = lambda *v: (C.c_int * len(v))(*v)
+    dbl = lambda *v: (C.c_double * len(v))(*v)
+    P = lambda a: C.cast(a, C.c_void_p)
+    nx, ny, bc = ints(64, 32), ints(64, 32), ints(1, 0)
+    assert L.fv_ensemble_create(0, P(nx), P(ny), None, P(bc), P(bc), 1, 3, 0.5, None, C.byref(e)) == 1
+    assert L.fv_ensemble_create(2, P(ints(64, 0)), P(ny), None, P(bc), P(bc), 1, 3, 0.5, None, C.byref(e)) == 1
+    assert b"positive" in L.fv_last_error()
+    assert L.fv_ensemble_create(2, P(nx), P(ny), None, P(ints(1, 9)), P(bc), 1, 3, 0.5, None, C.byref(e)) == 1
+    assert b"bc" in L.fv_last_error()
+    bounds = dbl(0, 1, 0, 1, 0, 1, 0.5, 0.5)  # the second member's y extent is empty
+    assert L.fv_ensemble_create(2, P(nx), P(ny), P(bounds), P(bc), P(bc), 1, 3, 0.5, None, C.byref(e)) == 1
+    assert b"empty domain" in L.fv_last_error()
+    assert L.fv_ensemble_create(2, P(nx), P(ny), None, P(bc), P(bc), 5, 3, 0.5, None, C.byref(e)) == 1
+    assert L.fv_ensemble_create(2, P(nx), P(ny), None, P(bc), P(bc), 1, 3, 0.0, None, C.byref(e)) == 1
+    if not torch.cuda.is_available():
+        assert L.fv_ensemble_create(2, P(nx), P(ny), None, P(bc), P(bc), 1, 3, 0.5, None, C.byref(e)) == 2
+        assert b"no CUDA device" in L.fv_last_error()
+    # the convolution kernels: unsupported shapes and missing buffers are rejected up front
+    dummy = C.c_void_p(16)  # never dereferenced: every call below fails its checks first
+    assert L.fvnet_conv3x3(0, 16, 32, 2, 8, 48, dummy, dummy, dummy, None, dummy, dummy, None, None, None) == 1
+    assert b"bad shape" in L.fv_last_error()
+    assert L.fvnet_conv3x3(0, 16, 32, 2, 8, 64, None, dummy, dummy, None, dummy, dummy, None, None, None) == 1
+    assert L.fvnet_conv3x3(0, 16, 32, 2, 8, 64, dummy, dummy, None, None, dummy, dummy, None, None, None) == 1
+    assert b"hidden needs" in L.fv_last_error()
+    assert L.fvnet_conv3x3(1, 32, 16, 2, 8, 64, dummy, dummy, dummy, None, None, None, None, None, None) == 1
+    assert b"output needs" in L.fv_last_error()
+    assert L.fvnet_conv3x3(9, 32, 32, 2, 8, 64, dummy, dummy, dummy, None, dummy, dummy, None, None, None) == 1
+    assert b"unsupported" in L.fv_last_error()
