@@ -11,9 +11,12 @@ if str(ROOT) not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
-    # libfv.so and the driver are build products, not tracked files: build them (a no-op when they are
-    # current) before any test module loads them, so that a fresh checkout collects cleanly
+    # libfv.so, the driver and the oracle's libraries are build products, not tracked files: build them
+    # (a no-op when they are current) before any test module loads them or checks for them at
+    # collection, so that a fresh checkout collects and runs every test
     importlib.import_module("neural-pde-surrogate_b200.build").build()
+    from oracle import build_oracle
+    build_oracle.build()
 
 
 @pytest.fixture(scope="session")
