@@ -172,6 +172,24 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, fami
             "coarse_retries": retried, "failed": failed}
 
 
+def equal_error(hyb, plains, horizons):
+    """The equal-error comparison at each horizon h (frames): the coarsest plain resolution whose L1
+    density error at frame h is at most the hybrid's, and the ratio of their GPU times per trajectory
+    (> 1: the hybrid is cheaper).  plain_n is None where no plain resolution is as accurate."""
+    per = {}
+    for h in horizons:
+        e = hyb["L1_per_frame"][h - 1]
+        as_good = [r for r in plains if r["L1_per_frame"][h - 1] <= e]
+        if as_good:
+            best = min(as_good, key=lambda r: r["n"])
+            per[h] = {"hybrid_L1": e, "plain_n": best["n"], "plain_L1": best["L1_per_frame"][h - 1],
+                      "plain_ms": best["ms_per_traj"], "hybrid_ms": hyb["ms_per_traj"],
+                      "speedup": best["ms_per_traj"] / hyb["ms_per_traj"]}
+        else:
+            per[h] = {"hybrid_L1": e, "plain_n": None}
+    return per
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--model", required=True)
@@ -204,18 +222,7 @@ def main():
     horizons = sorted({h for h in (5, 10, 20, a.frames) if h <= a.frames})
     summary["horizons"] = horizons
     for hyb in hybrids:
-        per = {}
-        for h in horizons:
-            e = hyb["L1_per_frame"][h - 1]
-            cheaper = [r for r in plains if r["L1_per_frame"][h - 1] <= e]
-            if cheaper:
-                best = min(cheaper, key=lambda r: r["n"])
-                per[h] = {"hybrid_L1": e, "plain_n": best["n"], "plain_L1": best["L1_per_frame"][h - 1],
-                          "plain_ms": best["ms_per_traj"], "hybrid_ms": hyb["ms_per_traj"],
-                          "speedup": best["ms_per_traj"] / hyb["ms_per_traj"]}
-            else:
-                per[h] = {"hybrid_L1": e, "plain_n": None}
-        summary["equal_error"][hyb["method"]] = per
+        summary["equal_error"][hyb["method"]] = equal_error(hyb, plains, horizons)
     print(f"{'method':18s} {'n':>5s} {'L1 final':>10s} {'L1 mean':>10s} {'ms/traj':>9s} {'drift m':>9s} {'drift E':>9s}"
           f" {'partial':>8s} {'retries':>7s}  L1 final by family")
     for r in rows:

@@ -159,3 +159,19 @@ def test_update_k_uses_optax_schedule_count_k_minus_one():
     assert tc.update_lr(1000, cfg) > 1e-5  # the end value is reached only at count = steps
     cfg_short = {"steps": 100, "lr": 2e-3, "warmup": 500}  # warm-up capped at half the steps
     assert tc.update_lr(51, cfg_short) == pytest.approx(2e-3)
+
+
+def test_equal_error_picks_the_coarsest_plain_grid_as_accurate_as_the_hybrid():
+    hyb = {"L1_per_frame": [0.02, 0.04, 0.06, 0.10], "ms_per_traj": 0.5}
+    plains = [{"n": 64, "L1_per_frame": [0.03, 0.05, 0.08, 0.105], "ms_per_traj": 0.3},
+              {"n": 128, "L1_per_frame": [0.02, 0.035, 0.05, 0.066], "ms_per_traj": 1.75},
+              {"n": 256, "L1_per_frame": [0.01, 0.018, 0.027, 0.036], "ms_per_traj": 11.5}]
+    per = pa.equal_error(hyb, plains, [1, 2, 4])
+    assert per[1]["plain_n"] == 128 and per[1]["plain_L1"] == 0.02  # ties count as as-accurate
+    assert per[2]["plain_n"] == 128 and per[2]["speedup"] == 1.75 / 0.5
+    assert per[4]["plain_n"] == 128 and per[4]["hybrid_ms"] == 0.5
+    worse = {"L1_per_frame": [0.001] * 4, "ms_per_traj": 0.5}
+    assert pa.equal_error(worse, plains, [3]) == {3: {"hybrid_L1": 0.001, "plain_n": None}}
+    cheap = {"L1_per_frame": [0.5] * 4, "ms_per_traj": 0.5}  # even plain 64^2 is better: speedup < 1
+    assert pa.equal_error(cheap, plains, [4])[4]["plain_n"] == 64
+    assert pa.equal_error(cheap, plains, [4])[4]["speedup"] == 0.3 / 0.5
