@@ -155,12 +155,16 @@ def reduce_over_ranks(ms, cells, launches, device):
     return float(t.item()), float(c[0].item()), int(c[1].item())
 
 
-def bench_config(n, world):
-    """The workload both arms report: the same keys and values for ours and the reference."""
-    return {"workload": f"blast+bubble {n}^2 FP64 periodic, t=0.2, 20 frames -> 128^2/64^2 f32, "
-                        f"4 flux x limiter combos per step", "grid": n, "frames": NOUT,
-            "combos": [f"{a}+{b}" for a, b in COMBOS], "parallelism": f"replicas x{world}",
-            "l2": "GPU arm: 256 MB buffer written before every step (state 8.4 MB is L2-resident within a step)"}
+def bench_config(n, world, build="parity"):
+    """The workload both arms report: the same keys and values for ours and the reference.  A run of
+    the tolerance build says so (the default parity build is bit-identical to the reference)."""
+    cfg = {"workload": f"blast+bubble {n}^2 FP64 periodic, t=0.2, 20 frames -> 128^2/64^2 f32, "
+                       f"4 flux x limiter combos per step", "grid": n, "frames": NOUT,
+           "combos": [f"{a}+{b}" for a, b in COMBOS], "parallelism": f"replicas x{world}",
+           "l2": "GPU arm: 256 MB buffer written before every step (state 8.4 MB is L2-resident within a step)"}
+    if build != "parity":
+        cfg["build"] = "tolerance: FMA contraction, within 1e-12 relative per step and 1e-9 per run of the parity build"
+    return cfg
 
 
 def run_ours(args):
@@ -268,7 +272,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded blast + bubble initial conditions)",
-        "config": bench_config(n, world),
+        "config": bench_config(n, world, args.build),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": f"stage_kernel<stage {stage}>", "achieved": achieved, "peak": peak,
@@ -377,7 +381,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-solver-steps", type=int, default=20)
+    ap.add_argument("--build", choices=["parity", "tolerance"], default="parity",
+                    help="solver library: the bit-exact parity build, or the FMA-contracted tolerance build")
     args = ap.parse_args()
+    os.environ["FV_BUILD"] = args.build  # read when the solver library is first loaded
     if args.impl == "reference":
         run_reference(args)
     else:

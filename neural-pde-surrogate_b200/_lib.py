@@ -1,6 +1,7 @@
 """ctypes loader for libfv.so (include/fv.h).  No CPU fallback: if the library or a GPU is missing,
 calls raise instead of computing anything elsewhere."""
 import ctypes as C
+import os
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -118,11 +119,18 @@ class StreamOrder:
             cur.wait_stream(ext)
 
 
+BUILDS = {"parity": "libfv.so", "tolerance": "libfv_tol.so"}
+
+
 def lib():
-    """The loaded libfv.so (raises if it has not been built)."""
+    """The loaded solver library (raises if it has not been built): libfv.so, the bit-exact parity
+    build, unless the environment sets FV_BUILD=tolerance (libfv_tol.so, FMA contraction)."""
     global _lib
     if _lib is None:
-        path = PKG / "libfv.so"
+        build = os.environ.get("FV_BUILD", "parity")
+        if build not in BUILDS:
+            raise ValueError(f"FV_BUILD={build!r}: use one of {', '.join(BUILDS)}")
+        path = PKG / BUILDS[build]
         if not path.exists():
             raise ImportError(f"{path} is missing: build it with `python {PKG / 'build.py'}` (nvcc, sm_100a)")
         L = C.CDLL(str(path))

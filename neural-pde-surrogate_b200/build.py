@@ -30,6 +30,9 @@ LIBS = {
         "headers": ["fv.h", "fvnet.h"],
     },
 }
+# The tolerance build: the same sources with FMA contraction, for the stated tolerances (1e-12 relative
+# per step, 1e-9 per run) instead of bit-exactness; loaded only when FV_BUILD=tolerance.
+LIBS["libfv_tol.so"] = {**LIBS["libfv.so"], "flags": ["--fmad=true", "-DFV_TOLERANCE_BUILD=1"]}
 
 
 def _stale(out, deps, headers):

@@ -369,7 +369,11 @@ int fv_internal_encode_maps(const GridDesc& g, int tx, int ty, TileMaps* out) { 
 extern "C" {
 
 const char* fv_last_error(void) { return g_last_error.c_str(); }
+#ifdef FV_TOLERANCE_BUILD
+const char* fv_version(void) { return "fv-b200 1.0 (sm_100a, FP64, tolerance build: FMA contraction)"; }
+#else
 const char* fv_version(void) { return "fv-b200 1.0 (sm_100a, FP64, bit-exact build)"; }
+#endif
 
 int fv_create(int nx, int ny, double x_min, double x_max, double y_min, double y_max, int bc_x, int bc_y,
               int flux, int limiter, double cfl, void* stream, fv_solver** out) {

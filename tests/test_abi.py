@@ -10,8 +10,8 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 PKG = ROOT / "neural-pde-surrogate_b200"
 
-# header -> shared library that implements it
-LIBS = {"fv.h": "libfv.so", "fvnet.h": "libfv.so"}
+# (header, shared library that implements it): the parity build and the tolerance build
+LIBS = [(h, lib) for lib in ("libfv.so", "libfv_tol.so") for h in ("fv.h", "fvnet.h")]
 
 
 def declared(header):
@@ -26,7 +26,7 @@ def built():
     importlib.import_module("neural-pde-surrogate_b200.build").build()
 
 
-@pytest.mark.parametrize("header,lib", sorted(LIBS.items()))
+@pytest.mark.parametrize("header,lib", LIBS)
 def test_library_exports_every_declared_symbol(header, lib):
     path = PKG / lib
     assert path.exists(), f"{lib} not built"
@@ -103,3 +103,22 @@ def test_ensemble_and_network_argument_validation_without_gpu(fvpkg):
     assert b"output needs" in L.fv_last_error()
     assert L.fvnet_conv3x3(9, 32, 32, 2, 8, 64, dummy, dummy, dummy, None, dummy, dummy, None, None, None) == 1
     assert b"unsupported" in L.fv_last_error()
+
+
+@pytest.mark.parametrize("build,marker", [(None, b"bit-exact build"), ("parity", b"bit-exact build"),
+                                          ("tolerance", b"tolerance build"), ("fast", None)])
+def test_fv_build_selects_the_library(build, marker):
+    """FV_BUILD picks the solver library when it is first loaded; unset means the bit-exact build."""
+    import os
+    import sys
+    env = {k: v for k, v in os.environ.items() if k != "FV_BUILD"}
+    if build:
+        env["FV_BUILD"] = build
+    code = ("import importlib, sys; sys.path.insert(0, sys.argv[1]); "
+            "print(importlib.import_module('neural-pde-surrogate_b200').lib().fv_version().decode())")
+    r = subprocess.run([sys.executable, "-c", code, str(ROOT)], capture_output=True, text=True, env=env, timeout=120)
+    if marker is None:
+        assert r.returncode != 0 and "use one of parity, tolerance" in r.stderr
+    else:
+        assert r.returncode == 0, r.stderr
+        assert marker.decode() in r.stdout

@@ -123,3 +123,9 @@ def test_clock_sampling_follows_the_device_mask(monkeypatch):
     monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "GPU-8f1e, GPU-77aa")
     assert bench.smi_id(1) == "GPU-77aa"
     assert bench.Clocks(0).index == "GPU-8f1e"
+
+
+def test_a_tolerance_build_run_says_so_in_its_config():
+    assert "build" not in bench.bench_config(512, 1)
+    assert bench.bench_config(512, 1, "tolerance")["build"].startswith("tolerance: FMA contraction")
+    assert {k: v for k, v in bench.bench_config(512, 1, "tolerance").items() if k != "build"} == bench.bench_config(512, 1)
