@@ -62,13 +62,34 @@ __device__ __forceinline__ double div_gm1(double p) {
     return fma(r, Y_GM1, q0);
 }
 
+// a / b at every general division site below: the IEEE quotient in the parity build.
+#ifndef FV_TOLERANCE_BUILD
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+#else
+// The tolerance build (FMA contraction; 1e-12 relative per step and 1e-9 per run of the parity build
+// allowed): a seed y ~ 1/b from the approximate reciprocal instruction, one Newton-Raphson step
+// y + y(1 - b y), q0 = a y, and Markstein's correction q0 + (a - q0 b) y (the method cited above).
+// Emulated on a CPU with seeds of relative error up to 2^-20 this gave the correctly rounded
+// quotient for all of 2e7 random operand pairs, and at most 1 ulp from 2^-14 seeds.  Operands
+// outside 2^-500 < |b| < 2^500, |a| < 2^500 (zeros, infinities, NaN, extremes) take `/`.
+__device__ __forceinline__ double fdiv(double a, double b) {
+    const double mb = fabs(b);
+    if (!(mb > 0x1p-500 && mb < 0x1p+500 && fabs(a) < 0x1p+500)) return a / b;
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    y = fma(y, fma(-b, y, 1.0), y);
+    const double q = a * y;
+    return fma(fma(-q, b, a), y, q);
+}
+#endif
+
 // a / b with a fast path for a zero numerator (zero velocities in a fluid at rest, equal left and
 // right states at a face): IEEE gives +-0 / b = +-0 with the sign of a XOR the sign of b for every
 // nonzero, non-NaN b (infinities included), which is a * copysign(1, b) exactly.  The general
 // division routine treats a zero numerator as a special case and runs ~3x slower on it.
 __device__ __forceinline__ double div_z(double a, double b) {
     if (a == 0.0 && b != 0.0 && b == b) return a * copysign(1.0, b);
-    return a / b;
+    return fdiv(a, b);
 }
 
 // state2d.hpp:16-19 (p / (GAMMA - 1.0) through div_gm1: same bits, fewer instructions)
@@ -84,7 +105,7 @@ __device__ __forceinline__ Q4 to_primitive(const Q4& U) {
 }
 
 // state2d.hpp:27
-__device__ __forceinline__ double sound_speed(const Q4& W) { return sqrt(GAMMA * W.d / W.a); }
+__device__ __forceinline__ double sound_speed(const Q4& W) { return sqrt(fdiv(GAMMA * W.d, W.a)); }
 
 // state2d.hpp:30-36, with the primitive state of U supplied by the caller (it is the same
 // to_primitive(U) the reference recomputes, so reusing it is bit-identical).
@@ -104,7 +125,7 @@ __device__ __forceinline__ double limiter(double a, double b) {
         return (fabs(a) < fabs(b)) ? a : b;
     } else {
         if (a * b <= 0.0) return 0.0;
-        return 2.0 * a * b / (a + b);
+        return fdiv(2.0 * a * b, a + b);
     }
 }
 
@@ -151,7 +172,7 @@ __device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& UR) {
     if (0.0 <= SL || !(left || 0.0 <= SR)) return F;   // pure upwind: F(UL) if 0<=SL, F(UR) if SR<0
     double factor = div_z(W.a * (S - W.b), S - S_star);
     Q4 st{factor, factor * S_star, factor * W.c,
-          factor * (U.d / W.a + (S_star - W.b) * (S_star + W.d / (W.a * (S - W.b))))};
+          factor * (fdiv(U.d, W.a) + (S_star - W.b) * (S_star + fdiv(W.d, W.a * (S - W.b))))};
     return Q4{F.a + S * (st.a - U.a), F.b + S * (st.b - U.b), F.c + S * (st.c - U.c), F.d + S * (st.d - U.d)};
 }
 
