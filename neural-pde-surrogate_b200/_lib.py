@@ -90,6 +90,38 @@ _PROTOS = {
 _lib = None
 
 
+def device_ptr(t, shape=None, numel=None, dtype="torch.float64", what="tensor"):
+    """Raw pointer of a CUDA tensor that a libfv call reads or writes whole.  The call trusts the
+    pointer for its full extent, so a wrong device, dtype, layout or size would make the kernel touch
+    memory outside the tensor: this checks all four and raises instead (not an assert, which
+    `python -O` would drop)."""
+    if not (hasattr(t, "data_ptr") and getattr(t, "is_cuda", False)):
+        raise TypeError(f"{what}: expected a CUDA tensor, got {type(t).__name__}")
+    if str(t.dtype) != dtype:
+        raise TypeError(f"{what}: expected dtype {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{what}: must be contiguous")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{what}: expected shape {tuple(shape)}, got {tuple(t.shape)}")
+    if numel is not None and t.numel() != numel:
+        raise ValueError(f"{what}: expected {numel} elements, got {t.numel()}")
+    return C.c_void_p(t.data_ptr())
+
+
+def host_out_ptr(a, shape, dtype, what="out"):
+    """Raw pointer of a caller's numpy array that a libfv call writes whole: the same checks as
+    device_ptr, for host memory."""
+    import numpy as np
+    if not isinstance(a, np.ndarray):
+        raise TypeError(f"{what}: expected a numpy array, got {type(a).__name__}")
+    if a.dtype != np.dtype(dtype) or a.shape != tuple(shape):
+        raise ValueError(f"{what}: expected a {np.dtype(dtype)} array of shape {tuple(shape)}, "
+                         f"got {a.dtype} {a.shape}")
+    if not (a.flags.c_contiguous and a.flags.writeable):
+        raise ValueError(f"{what}: must be C-contiguous and writeable")
+    return C.c_void_p(a.ctypes.data)
+
+
 class StreamOrder:
     """Orders a library handle's CUDA stream against torch's current stream.  The library queues the
     *_device copies on its own non-blocking stream, which nothing orders against torch's work: a

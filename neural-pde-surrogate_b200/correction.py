@@ -26,7 +26,7 @@ import math
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import check, device_ptr, lib
 
 CORR_MODES = {"strict": 0, "keep": 1, "scale": 2}  # FVNET_CORR_* of include/fvnet.h
 
@@ -72,7 +72,8 @@ class CorrectionNet:
                     chunks += [g.uniform(-lim, lim, co * ci * 9), g.uniform(-lim, lim, co)]
             params = np.concatenate(chunks).astype(np.float32)
         self.params = torch.as_tensor(np.asarray(params, np.float32), device=device).contiguous()
-        assert self.params.numel() == n
+        if self.params.numel() != n:
+            raise ValueError(f"params: expected {n} values, got {self.params.numel()}")
         self.grads = torch.zeros_like(self.params)
         self.m = torch.zeros_like(self.params)
         self.v = torch.zeros_like(self.params)
@@ -127,7 +128,8 @@ class CorrectionNet:
         """U: (B, H, W, 4) float64 CUDA state -> self.out4 (B, H, W, 4) float32 network output."""
         L, st = lib(), self.stream()
         B, H, W = self.B, self.H, self.W
-        check(L.fvnet_prep_input(_p(U), self.npix, _p(stats), _p(self.X16), st))
+        Up = device_ptr(U, (B, H, W, 4), what="U")
+        check(L.fvnet_prep_input(Up, self.npix, device_ptr(stats, numel=8, what="stats"), _p(self.X16), st))
         x = self.X16
         for k in range(5):
             cip, cop = LAYERS[k][2], LAYERS[k][3]
@@ -142,6 +144,8 @@ class CorrectionNet:
         """Gradients of all parameters into self.grads from d loss / d out (B, H, W, 16) BF16."""
         L, st = lib(), self.stream()
         B, H, W = self.B, self.H, self.W
+        if dout16 is not None:
+            device_ptr(dout16, (B, H, W, 16), dtype="torch.bfloat16", what="dout16")
         dz = self.dout16 if dout16 is None else dout16
         for k in range(5, -1, -1):
             ci, co, cip, cop = LAYERS[k]
@@ -170,15 +174,24 @@ class CorrectionNet:
         largest fraction theta of the correction that keeps rho and p positive (self.theta);
         'keep' -> always the full correction (the trained step of a training iteration)."""
         self.forward(Uc, stats)
-        check(lib().fvnet_apply_correction(_p(Uc), _p(self.out4), self.B, self.H * self.W, _p(dscale), _p(Unext),
-                                           _p(fallback), _p(self.theta), CORR_MODES[mode], self.stream()))
+        shape = (self.B, self.H, self.W, 4)
+        check(lib().fvnet_apply_correction(device_ptr(Uc, shape, what="Uc"), _p(self.out4), self.B, self.H * self.W,
+                                           device_ptr(dscale, numel=4, what="dscale"),
+                                           device_ptr(Unext, shape, what="Unext"),
+                                           device_ptr(fallback, (self.B,), dtype="torch.int32", what="fallback"),
+                                           _p(self.theta), CORR_MODES[mode], self.stream()))
         return Unext
 
     def loss_grad(self, Unext, Y, Uc, stats, dscale, theta, loss_part):
         """Uc: the coarse state the correction was added to; theta: per-sample fraction of the
         correction applied (gradient scale), or None (1)."""
-        check(lib().fvnet_loss_grad(_p(Unext), _p(Y), _p(Uc), self.B, self.H * self.W, _p(stats), _p(dscale),
-                                    _p(theta), _p(loss_part), _p(self.dout16), self.stream()))
+        shape = (self.B, self.H, self.W, 4)
+        th = None if theta is None else device_ptr(theta, (self.B,), what="theta")
+        check(lib().fvnet_loss_grad(device_ptr(Unext, shape, what="Unext"), device_ptr(Y, shape, what="Y"),
+                                    device_ptr(Uc, shape, what="Uc"), self.B, self.H * self.W,
+                                    device_ptr(stats, numel=8, what="stats"), device_ptr(dscale, numel=4, what="dscale"),
+                                    th, device_ptr(loss_part, (self.B,), what="loss_part"), _p(self.dout16),
+                                    self.stream()))
         return loss_part
 
 

@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import FV_ERR_NONPHYSICAL, FVError, StreamOrder, check, lib
+from ._lib import FV_ERR_NONPHYSICAL, FVError, StreamOrder, check, device_ptr, lib
 from .solver import FLUXES, LIMITERS
 
 
@@ -47,9 +47,9 @@ class Ensemble:
     def set_state(self, k, U):
         g = self.grids[k]
         if hasattr(U, "data_ptr") and getattr(U, "is_cuda", False):
-            assert tuple(U.shape) == (g.ny, g.nx, 4) and U.is_contiguous()
+            ptr = device_ptr(U, (g.ny, g.nx, 4), what=f"member {k} state")
             self._order.before()
-            check(lib().fv_ensemble_set_state_device(self._h, int(k), C.c_void_p(U.data_ptr())))
+            check(lib().fv_ensemble_set_state_device(self._h, int(k), ptr))
             return
         U = np.ascontiguousarray(U, np.float64)
         if U.shape != (g.ny, g.nx, 4):
@@ -59,17 +59,15 @@ class Ensemble:
     def set_all(self, U):
         """All members from one CUDA float64 tensor holding their states back to back in member order
         (e.g. shape (count, ny, nx, 4) when all members have one size)."""
-        assert getattr(U, "is_cuda", False) and U.is_contiguous() and str(U.dtype) == "torch.float64"
-        assert U.numel() == 4 * sum(g.nx * g.ny for g in self.grids)
+        ptr = device_ptr(U, numel=4 * sum(g.nx * g.ny for g in self.grids), what="states")
         self._order.before()  # U may still be being written on torch's stream
-        check(lib().fv_ensemble_set_all_device(self._h, C.c_void_p(U.data_ptr())))
+        check(lib().fv_ensemble_set_all_device(self._h, ptr))
 
     def get_all(self, out):
         """All members' states into a CUDA float64 tensor (layout of set_all)."""
-        assert getattr(out, "is_cuda", False) and out.is_contiguous() and str(out.dtype) == "torch.float64"
-        assert out.numel() == 4 * sum(g.nx * g.ny for g in self.grids)
+        ptr = device_ptr(out, numel=4 * sum(g.nx * g.ny for g in self.grids), what="out")
         self._order.before()  # torch may still be reading out's previous contents
-        check(lib().fv_ensemble_get_all_device(self._h, C.c_void_p(out.data_ptr())))
+        check(lib().fv_ensemble_get_all_device(self._h, ptr))
         self._order.after()  # torch work on out waits for the copy
         return out
 

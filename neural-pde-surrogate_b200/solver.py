@@ -19,7 +19,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import BadCell, StreamOrder, check, lib
+from ._lib import BadCell, StreamOrder, check, device_ptr, host_out_ptr, lib
 
 FLUXES = {"rusanov": 0, "hllc": 1}            # main2d.cpp:145-148
 LIMITERS = {"none": 0, "unlimited": 1, "minmod": 2, "vanleer": 3}  # main2d.cpp:150-155
@@ -70,10 +70,6 @@ def _ptr(a):
     return C.c_void_p(a.ctypes.data)
 
 
-def _dev_ptr(t):
-    return C.c_void_p(t.data_ptr())
-
-
 class Solver:
     """Solver(grid, flux, limiter, cfl): flux in {'hllc','rusanov'}, limiter in {'none','minmod',
     'vanleer','unlimited'} (the driver's option names, main2d.cpp:25-28)."""
@@ -111,9 +107,9 @@ class Solver:
     def set_state(self, U):
         """U: host ndarray (ny, nx, 4) float64, or a CUDA torch tensor of that shape."""
         if hasattr(U, "data_ptr") and getattr(U, "is_cuda", False):
-            assert tuple(U.shape) == self.shape and U.is_contiguous() and str(U.dtype) == "torch.float64"
+            ptr = device_ptr(U, self.shape, what="state")
             self._order().before()
-            check(lib().fv_set_state_device(self._h, _dev_ptr(U)))
+            check(lib().fv_set_state_device(self._h, ptr))
             return
         U = np.ascontiguousarray(U, dtype=np.float64)
         if U.shape != self.shape:
@@ -134,12 +130,13 @@ class Solver:
 
     def get_state(self, out=None):
         if out is not None and hasattr(out, "data_ptr") and getattr(out, "is_cuda", False):
+            ptr = device_ptr(out, self.shape, what="out")
             self._order().before()
-            check(lib().fv_get_state_device(self._h, _dev_ptr(out)))
+            check(lib().fv_get_state_device(self._h, ptr))
             self._order().after()
             return out
         out = np.empty(self.shape, np.float64) if out is None else out
-        check(lib().fv_get_state(self._h, _ptr(out)))
+        check(lib().fv_get_state(self._h, host_out_ptr(out, self.shape, np.float64)))
         return out
 
     def set_time(self, t):
@@ -180,12 +177,13 @@ class Solver:
         """trajectory.hpp:31-51 for one level: (4, ny/f, nx/f) float32."""
         shape = (4, self.grid.ny // factor, self.grid.nx // factor)
         if out is not None and hasattr(out, "data_ptr") and getattr(out, "is_cuda", False):
+            ptr = device_ptr(out, shape, dtype="torch.float32", what="out")
             self._order().before()
-            check(lib().fv_block_average_device(self._h, int(factor), _dev_ptr(out)))
+            check(lib().fv_block_average_device(self._h, int(factor), ptr))
             self._order().after()
             return out
         out = np.empty(shape, np.float32) if out is None else out
-        check(lib().fv_block_average(self._h, int(factor), _ptr(out)))
+        check(lib().fv_block_average(self._h, int(factor), host_out_ptr(out, shape, np.float32)))
         return out
 
     def run_trajectory(self, t_end, t_start=0.0, nout=1, sizes=None):
@@ -215,7 +213,8 @@ def riemann_flux(flux, UL, UR, face="x"):
     UL, UR: (..., 4) conserved states; returns F of the same shape."""
     UL = np.ascontiguousarray(UL, np.float64)
     UR = np.ascontiguousarray(UR, np.float64)
-    assert UL.shape == UR.shape and UL.shape[-1] == 4
+    if UL.shape != UR.shape or UL.ndim == 0 or UL.shape[-1] != 4:
+        raise ValueError(f"UL and UR must have the same shape (..., 4), got {UL.shape} and {UR.shape}")
     F = np.empty_like(UL)
     check(lib().fv_riemann_flux(FLUXES[flux], 1 if face == "y" else 0, UL.size // 4, _ptr(UL), _ptr(UR), _ptr(F)))
     return F
@@ -224,6 +223,8 @@ def riemann_flux(flux, UL, UR, face="x"):
 def fill_ghosts(U, bc_x, bc_y):
     """(ny+4, nx+4, 4) ghosted array apply_bcs would build (grid2d.hpp:43-66), made on the GPU."""
     U = np.ascontiguousarray(U, np.float64)
+    if U.ndim != 3 or U.shape[2] != 4:
+        raise ValueError(f"U must have shape (ny, nx, 4), got {U.shape}")
     ny, nx = U.shape[:2]
     bc_x = BC.names[bc_x] if isinstance(bc_x, str) else int(bc_x)
     bc_y = BC.names[bc_y] if isinstance(bc_y, str) else int(bc_y)

@@ -122,3 +122,61 @@ def test_fv_build_selects_the_library(build, marker):
     else:
         assert r.returncode == 0, r.stderr
         assert marker.decode() in r.stdout
+
+
+class _FakeCudaTensor:
+    """Enough of a CUDA tensor's surface for the pointer checks (no device needed)."""
+
+    def __init__(self, shape, dtype="torch.float64", contiguous=True):
+        import math
+        self.shape, self.dtype, self._contig, self.is_cuda = tuple(shape), dtype, contiguous, True
+        self._numel = math.prod(shape)
+
+    def is_contiguous(self):
+        return self._contig
+
+    def numel(self):
+        return self._numel
+
+    def data_ptr(self):
+        return 4096
+
+
+def test_pointer_checks_reject_what_a_kernel_would_overrun():
+    import numpy as np
+    from importlib import import_module
+    L = import_module("neural-pde-surrogate_b200._lib")
+    assert L.device_ptr(_FakeCudaTensor((2, 8, 8, 4)), (2, 8, 8, 4)).value == 4096
+    assert L.device_ptr(_FakeCudaTensor((3,), "torch.int32"), (3,), dtype="torch.int32").value == 4096
+    assert L.device_ptr(_FakeCudaTensor((2, 4)), numel=8).value == 4096
+    with pytest.raises(ValueError, match="expected shape"):
+        L.device_ptr(_FakeCudaTensor((2, 8, 8, 3)), (2, 8, 8, 4))
+    with pytest.raises(TypeError, match="dtype torch.float64"):
+        L.device_ptr(_FakeCudaTensor((2, 8, 8, 4), "torch.float32"), (2, 8, 8, 4))
+    with pytest.raises(ValueError, match="contiguous"):
+        L.device_ptr(_FakeCudaTensor((2, 8, 8, 4), contiguous=False), (2, 8, 8, 4))
+    with pytest.raises(ValueError, match="expected 12 elements"):
+        L.device_ptr(_FakeCudaTensor((2, 4)), numel=12)
+    with pytest.raises(TypeError, match="CUDA tensor"):
+        L.device_ptr(np.zeros(4), numel=4)
+    import torch
+    with pytest.raises(TypeError, match="CUDA tensor"):
+        L.device_ptr(torch.zeros(4, dtype=torch.float64), numel=4)  # a CPU tensor
+    out = np.empty((4, 2, 2), np.float32)
+    assert L.host_out_ptr(out, (4, 2, 2), np.float32).value == out.ctypes.data
+    with pytest.raises(ValueError, match="float32 array of shape"):
+        L.host_out_ptr(np.empty((4, 2, 2), np.float64), (4, 2, 2), np.float32)
+    with pytest.raises(ValueError, match="float64 array of shape"):
+        L.host_out_ptr(np.empty((3, 3, 4)), (3, 4, 4), np.float64)
+    with pytest.raises(ValueError, match="C-contiguous"):
+        L.host_out_ptr(np.empty((4, 4, 4))[:, ::2], (4, 2, 4), np.float64)
+    with pytest.raises(TypeError, match="numpy array"):
+        L.host_out_ptr([0.0] * 4, (4,), np.float64)
+
+
+def test_host_helpers_check_shapes_before_calling_the_library(fvpkg):
+    import numpy as np
+    with pytest.raises(ValueError, match="same shape"):
+        fvpkg.riemann_flux("hllc", np.ones((3, 4)), np.ones((2, 4)))
+    with pytest.raises(ValueError, match=r"\(ny, nx, 4\)"):
+        fvpkg.fill_ghosts(np.ones((4, 4, 3)), "periodic", "periodic")
