@@ -130,3 +130,17 @@ def kh_growth_rate(make, n, nout=20, t_end=2.0, window=(0.6, 1.2)):
     ts, amps = np.array(ts), np.array(amps)
     sel = (ts >= window[0] - 1e-12) & (ts <= window[1] + 1e-12)
     return float(np.polyfit(ts[sel], np.log(amps[sel]), 1)[0]), amps
+
+
+def sine2d_l1(make, n, limiter):
+    """experiments/results.md section 3 (2D diagonal advection, HLLC, CFL 0.5, t = 1): the L1 density
+    error against the exact solution sampled at cell centres, sum |err| dx dy, as
+    experiments/convergence_sine2d.py:18-26 computes it; one run to t = 1."""
+    g, t_end, U0 = ic.test_problem("sine2d", n)
+    s = make(g, "hllc", limiter, 0.5)
+    s.set_state(U0)
+    run_to(s, t_end)
+    x = ic.cell_centres(n)
+    X, Y = np.meshgrid(x, x)
+    exact = 1.0 + 0.2 * np.sin(2.0 * np.pi * (X + Y - 2.0 * t_end))
+    return float(np.abs(s.get_state()[..., 0] - exact).sum() * (x[1] - x[0]) * (x[1] - x[0]))

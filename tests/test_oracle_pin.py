@@ -208,3 +208,12 @@ def test_kh_growth_rates_match_the_reference_validation():
         rate, amps = ka.kh_growth_rate(mk, n)
         assert abs(rate - published) < 0.01, (n, rate, published)
         assert amps[0] == pytest.approx(0.01)  # the seeded amplitude, v = 0.01 sin(4 pi x)
+
+
+@pytest.mark.parametrize("n,limiter,published", [(32, "none", "9.024e-02"), (32, "vanleer", "1.088e-02"),
+                                                 (64, "none", "5.862e-02"), (64, "vanleer", "3.203e-03"),
+                                                 (128, "none", "3.379e-02"), (128, "vanleer", "8.531e-04")])
+def test_sine2d_errors_match_the_published_table(n, limiter, published):
+    """experiments/results.md section 3: the reference's published L1 errors, to every printed digit."""
+    mk = lambda g, f, l, c: cpu_solver("oracle", g, f, l, c)
+    assert f"{ka.sine2d_l1(mk, n, limiter):.3e}" == published
