@@ -144,3 +144,20 @@ def sine2d_l1(make, n, limiter):
     X, Y = np.meshgrid(x, x)
     exact = 1.0 + 0.2 * np.sin(2.0 * np.pi * (X + Y - 2.0 * t_end))
     return float(np.abs(s.get_state()[..., 0] - exact).sum() * (x[1] - x[0]) * (x[1] - x[0]))
+
+
+def kh_final_amplitude(make, n, nout=20):
+    """experiments/results.md:98-102: the seeded KH mode's amplitude at the driver's end time t = 2
+    (the `kh` test, HLLC + van Leer, frames every t_end / nout)."""
+    g, t_end, U0 = ic.test_problem("kh", n)
+    s = make(g, "hllc", "vanleer", 0.5)
+    s.set_state(U0)
+    t = 0.0
+    for k in range(1, nout + 1):
+        t_next = 0.0 + ((t_end - 0.0) * k) / nout
+        while t < t_next:
+            dt = s.compute_dt()
+            dt = (t_next - t) if (t_next - t) < dt else dt
+            s.step(dt)
+            t += dt
+    return kh_mode_amplitude(s.get_state(), n)

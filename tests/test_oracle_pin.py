@@ -201,13 +201,16 @@ def test_exact_sod_star_state():
 
 def test_kh_growth_rates_match_the_reference_validation():
     """README.md:66-69 / experiments/results.md:98-102: the seeded KH mode decays at 16^2 and grows at
-    1.20, 2.41 and 2.71 at 32^2, 64^2 and 128^2 (HLLC + van Leer, fit over 0.6 <= t <= 1.2)."""
+    1.20, 2.41 and 2.71 at 32^2, 64^2 and 128^2 (HLLC + van Leer, fit over 0.6 <= t <= 1.2); its
+    amplitude at t = 2 is 0.193 at 64^2 and 0.225 at 128^2."""
     mk = lambda g, f, l, c: cpu_solver("oracle", g, f, l, c)
     assert ka.kh_growth_rate(mk, 16)[0] < 0.0
     for n, published in ((32, 1.20), (64, 2.41), (128, 2.71)):
         rate, amps = ka.kh_growth_rate(mk, n)
         assert abs(rate - published) < 0.01, (n, rate, published)
         assert amps[0] == pytest.approx(0.01)  # the seeded amplitude, v = 0.01 sin(4 pi x)
+    for n, published in ((64, "0.193"), (128, "0.225")):  # the final mode amplitude at t = 2
+        assert f"{ka.kh_final_amplitude(mk, n):.3f}" == published
 
 
 @pytest.mark.parametrize("n,limiter,published", [(32, "none", "9.024e-02"), (32, "vanleer", "1.088e-02"),
