@@ -140,6 +140,32 @@ def test_init_file_missing_attribute(exe, tmp_path):
     assert r.returncode == 1 and "missing attribute nx" in r.stderr
 
 
+def _ic_arrays(n=8, rho=None):
+    one = np.ones((n, n))
+    return dict(rho=one if rho is None else rho, u=0 * one, v=0 * one, p=one, nx=np.int32(n), ny=np.int32(n),
+                x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, bc_x=np.array("periodic"),
+                bc_y=np.array("periodic"), t_end=np.float64(0.1), test=np.array("riemann"))
+
+
+def test_malformed_init_files_fail_cleanly(exe, tmp_path):
+    """Every unreadable IC file ends the driver with status 1 and a message, before any GPU work."""
+    import zipfile
+    (tmp_path / "garbage.npz").write_bytes(b"garbage")
+    np.savez(tmp_path / "full.npz", **_ic_arrays())
+    whole = (tmp_path / "full.npz").read_bytes()
+    (tmp_path / "truncated.npz").write_bytes(whole[: len(whole) // 2])
+    np.savez(tmp_path / "shape.npz", **_ic_arrays(rho=np.ones((4, 8))))
+    np.savez(tmp_path / "dtype.npz", **_ic_arrays(rho=np.ones((8, 8), np.complex128)))
+    with zipfile.ZipFile(tmp_path / "header.npz", "w") as z:
+        z.writestr("rho.npy", b"\x93NUMPY\x01\x00\x10\x00{'descr': '<f8',   ")
+    expected = {"garbage": "is not an .npz archive", "truncated": "is not an .npz archive",
+                "shape": "dataset rho has the wrong size", "dtype": "unsupported dtype <c16",
+                "header": ".npy header lacks fortran_order"}
+    for name, msg in expected.items():
+        r = run(exe, "--init", tmp_path / f"{name}.npz")
+        assert r.returncode == 1 and msg in r.stderr, (name, r.returncode, r.stderr)
+
+
 # ---------------------------------------------------------------- GPU: bit-identical runs
 
 
