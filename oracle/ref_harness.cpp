@@ -12,7 +12,6 @@
 #include "solver2d.hpp"
 #include "riemann.hpp"   // 1D flux, the comparison used by the reference's test_riemann2d.cpp
 
-#include <cstring>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -58,6 +57,10 @@ bool first_bad(const RefRun& r, int* bi, int* bj, double* brho, double* bp) {
 
 extern "C" {
 
+// one cell between the harness's flat (rho, rho*u, rho*v, E) doubles and the reference's Conserved
+static e2d::Conserved load_c(const double* p) { return e2d::Conserved{p[0], p[1], p[2], p[3]}; }
+static void store_c(double* p, const e2d::Conserved& c) { p[0] = c.rho; p[1] = c.mx; p[2] = c.my; p[3] = c.E; }
+
 void* ref_create(int nx, int ny, double x_min, double x_max, double y_min, double y_max, int bc_x, int bc_y,
                  int flux, int lim, double cfl) {
     auto* r = new RefRun;
@@ -74,14 +77,14 @@ void ref_set_state(void* h, const double* U) {
     auto* r = static_cast<RefRun*>(h);
     for (int j = 0; j < r->g.ny; ++j)
         for (int i = 0; i < r->g.nx; ++i)
-            std::memcpy(&r->U[r->g.idx(i, j)], U + (size_t(j) * r->g.nx + i) * 4, 32);
+            r->U[r->g.idx(i, j)] = load_c(U + (size_t(j) * r->g.nx + i) * 4);
 }
 
 void ref_get_state(void* h, double* U) {
     auto* r = static_cast<RefRun*>(h);
     for (int j = 0; j < r->g.ny; ++j)
         for (int i = 0; i < r->g.nx; ++i)
-            std::memcpy(U + (size_t(j) * r->g.nx + i) * 4, &r->U[r->g.idx(i, j)], 32);
+            store_c(U + (size_t(j) * r->g.nx + i) * 4, r->U[r->g.idx(i, j)]);
 }
 
 int ref_compute_dt(void* h, double* dt, int* bi, int* bj, double* brho, double* bp) {
@@ -131,25 +134,17 @@ void ref_apply_bcs_ghosted(int nx, int ny, int bc_x, int bc_y, double* Ug) {
     e2d::Grid g = e2d::make_grid(nx, ny, 0.0, 1.0, 0.0, 1.0, bc_x ? e2d::BC::Periodic : e2d::BC::Transmissive,
                                  bc_y ? e2d::BC::Periodic : e2d::BC::Transmissive);
     std::vector<e2d::Conserved> U(g.size());
-    std::memcpy(U.data(), Ug, sizeof(e2d::Conserved) * U.size());
+    for (size_t k = 0; k < U.size(); ++k) U[k] = load_c(Ug + 4 * k);
     e2d::apply_bcs(g, U);
-    std::memcpy(Ug, U.data(), sizeof(e2d::Conserved) * U.size());
+    for (size_t k = 0; k < U.size(); ++k) store_c(Ug + 4 * k, U[k]);
 }
 
 void ref_flux(int flux, const double* UL, const double* UR, double* F) {
-    e2d::Conserved a, b;
-    std::memcpy(&a, UL, 32);
-    std::memcpy(&b, UR, 32);
-    e2d::Conserved c = pick_flux(flux)(a, b);
-    std::memcpy(F, &c, 32);
+    store_c(F, pick_flux(flux)(load_c(UL), load_c(UR)));
 }
 
 void ref_flux_y(int flux, const double* UL, const double* UR, double* F) {
-    e2d::Conserved a, b;
-    std::memcpy(&a, UL, 32);
-    std::memcpy(&b, UR, 32);
-    e2d::Conserved c = e2d::flux_y_face(pick_flux(flux), a, b);
-    std::memcpy(F, &c, 32);
+    store_c(F, e2d::flux_y_face(pick_flux(flux), load_c(UL), load_c(UR)));
 }
 
 void ref_hllc_1d(const double* UL, const double* UR, double* F) {
