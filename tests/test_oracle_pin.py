@@ -220,3 +220,15 @@ def test_sine2d_errors_match_the_published_table(n, limiter, published):
     """experiments/results.md section 3: the reference's published L1 errors, to every printed digit."""
     mk = lambda g, f, l, c: cpu_solver("oracle", g, f, l, c)
     assert f"{ka.sine2d_l1(mk, n, limiter):.3e}" == published
+
+
+def test_lax_liu3_symmetric_to_the_published_level():
+    """README.md:64: Lax-Liu configuration 3 at 256^2, t = 0.3 (HLLC + van Leer) is symmetric about
+    x = y to 3e-14 (density; the oracle gives 2.4e-14)."""
+    g, t_end, U0 = ka.ic.test_problem("lax_liu3", 256)
+    s = cpu_solver("oracle", g, "hllc", "vanleer", 0.5)
+    s.set_state(U0)
+    s.advance_to(t_end)
+    U = s.get_state()
+    assert t_end == 0.3 and np.abs(U[..., 0] - U[..., 0].T).max() < 3e-14
+    assert max(np.abs(U[..., 1] - U[..., 2].T).max(), np.abs(U[..., 3] - U[..., 3].T).max()) < 1e-13
