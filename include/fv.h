@@ -147,6 +147,12 @@ int fv_ensemble_get_stream(fv_ensemble* e, void** stream);
  * Inspection hook for the Riemann solvers (the reference's test_riemann2d.cpp calls them directly). */
 int fv_riemann_flux(int flux, int y_face, int n, const double* UL, const double* UR, double* F);
 
+/* q[k] = a[k] / b[k] for n host doubles, computed on the GPU by the division the stage kernels use
+ * at every general division site: IEEE division in libfv.so; in the tolerance build (libfv_tol.so)
+ * a Newton-Raphson reciprocal with Markstein's correction.  Checks the tolerance build's division
+ * against IEEE on chosen operands. */
+int fv_eval_division(int n, const double* a, const double* b, double* q);
+
 /* The (ny+4) x (nx+4) ghosted array that apply_bcs (grid2d.hpp:43-66) builds from the interior
  * state U, produced on the GPU with the boundary mapping the stage kernels use (no ghost ring is
  * stored by the solver itself).  Ug: host array of (ny+4)*(nx+4)*4 doubles. */

@@ -684,6 +684,34 @@ int fv_riemann_flux(int flux, int y_face, int n, const double* UL, const double*
     return FV_OK;
 }
 
+}  // extern "C"
+
+// q[k] = a[k] / b[k] by the division every general division site of the stage kernels uses (fdiv).
+static __global__ void division_kernel(int n, const double* __restrict__ a, const double* __restrict__ b,
+                                       double* __restrict__ q) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) q[k] = fv::fdiv(a[k], b[k]);
+}
+
+extern "C" {
+
+int fv_eval_division(int n, const double* a, const double* b, double* q) {
+    if (n < 0 || (n > 0 && (!a || !b || !q))) return set_error(FV_ERR_ARG, "fv_eval_division: bad arguments");
+    if (n == 0) return FV_OK;
+    double* d = nullptr;
+    const size_t bytes = size_t(n) * sizeof(double);
+    FV_CUDA(cudaMalloc(&d, 3 * bytes));
+    cudaError_t e = cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + n, b, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        division_kernel<<<std::min((n + 255) / 256, 148 * 8), 256>>>(n, d, d + n, d + 2 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(q, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_error(FV_ERR_CUDA, "fv_eval_division: %s", cudaGetErrorString(e));
+    return FV_OK;
+}
+
 int fv_fill_ghosts(int nx, int ny, int bc_x, int bc_y, const double* U, double* Ug) {
     if (nx <= 0 || ny <= 0 || !U || !Ug) return set_error(FV_ERR_ARG, "fv_fill_ghosts: bad arguments");
     if (!valid_common(FLUX_HLLC, LIM_NONE, bc_x, bc_y)) return set_error(FV_ERR_ARG, "fv_fill_ghosts: unknown bc");

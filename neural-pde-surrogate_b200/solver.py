@@ -220,6 +220,19 @@ def riemann_flux(flux, UL, UR, face="x"):
     return F
 
 
+def eval_division(a, b):
+    """a / b elementwise, computed on the GPU by the division the stage kernels use at every general
+    division site (fv_eval_division): IEEE in the parity build, the Newton-Raphson sequence in the
+    tolerance build."""
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    if a.shape != b.shape:
+        raise ValueError(f"a and b must have the same shape, got {a.shape} and {b.shape}")
+    q = np.empty_like(a)
+    check(lib().fv_eval_division(a.size, _ptr(a), _ptr(b), _ptr(q)))
+    return q
+
+
 def fill_ghosts(U, bc_x, bc_y):
     """(ny+4, nx+4, 4) ghosted array apply_bcs would build (grid2d.hpp:43-66), made on the GPU."""
     U = np.ascontiguousarray(U, np.float64)

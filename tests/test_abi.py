@@ -180,3 +180,17 @@ def test_host_helpers_check_shapes_before_calling_the_library(fvpkg):
         fvpkg.riemann_flux("hllc", np.ones((3, 4)), np.ones((2, 4)))
     with pytest.raises(ValueError, match=r"\(ny, nx, 4\)"):
         fvpkg.fill_ghosts(np.ones((4, 4, 3)), "periodic", "periodic")
+
+
+def test_division_check_entry_point_without_gpu(fvpkg):
+    import numpy as np
+    import torch
+    L = fvpkg.lib()
+    assert L.fv_eval_division(-1, None, None, None) == 1 and b"bad arguments" in L.fv_last_error()
+    assert L.fv_eval_division(3, None, None, None) == 1
+    assert L.fv_eval_division(0, None, None, None) == 0  # nothing to do
+    with pytest.raises(ValueError, match="same shape"):
+        fvpkg.eval_division(np.ones(3), np.ones(4))
+    if not torch.cuda.is_available():
+        with pytest.raises(fvpkg.FVError):  # computed on the GPU or not at all
+            fvpkg.eval_division(np.ones(3), np.full(3, 3.0))
