@@ -18,5 +18,5 @@ def test_reference_solver_test_passes_on_the_gpu(cuda_ok):
         pytest.fail(f"{EXE} not built (the reference tree was absent when oracle/build_oracle.py ran)")
     r = subprocess.run([str(EXE)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("PASS") == 10 and "FAIL" not in r.stdout.replace("ALL PASSED", "")
+    assert r.stdout.count(" PASS  (") == 10 and " FAIL  (" not in r.stdout  # the program's ten checks
     assert "ALL PASSED (0 failures)" in r.stdout
