@@ -153,6 +153,27 @@ int fv_riemann_flux(int flux, int y_face, int n, const double* UL, const double*
  * against IEEE on chosen operands. */
 int fv_eval_division(int n, const double* a, const double* b, double* q);
 
+/* Division sequences of the stage kernels, for checking them against IEEE division (the reference
+ * divides with the IEEE `/` of its CPU build).  Where the parity build replaces `/` it is by a
+ * sequence that returns the same correctly rounded quotient:
+ *   FV_DIV_GENERAL  a / b at every general division site (IEEE `/` in libfv.so; a Newton-Raphson
+ *                   reciprocal with Markstein's correction in libfv_tol.so)
+ *   FV_DIV_GM1      a / (GAMMA - 1) (to_conserved, state2d.hpp:17); b is ignored and may be NULL
+ *   FV_DIV_ZERO     a / b with a fast path for a zero numerator (to_primitive, state2d.hpp:22-23)
+ *   FV_DIV_BACK     RN(RN(a*b) / a): with a = rho and b = u, the velocity to_primitive recovers from
+ *                   a face state's momentum (riemann2d.hpp:12,28 on to_conserved(edge), solver2d.hpp:145-148)
+ * fv_eval_division_kind evaluates one kind on n host operand pairs.  fv_division_sweep draws n
+ * operand pairs on the device (normal numbers near 1 and across the exponent range, zeros,
+ * subnormals, infinities, edge mantissas; seeded) and counts the quotients that differ in any bit from
+ * IEEE division, with the largest difference in ulps (max_ulps may be NULL).  No reference
+ * counterpart (the reference's divisions are its compiler's). */
+#define FV_DIV_GENERAL 0
+#define FV_DIV_GM1 1
+#define FV_DIV_ZERO 2
+#define FV_DIV_BACK 3
+int fv_eval_division_kind(int kind, int n, const double* a, const double* b, double* q);
+int fv_division_sweep(int kind, long long n, unsigned long long seed, long long* mismatches, long long* max_ulps);
+
 /* The (ny+4) x (nx+4) ghosted array that apply_bcs (grid2d.hpp:43-66) builds from the interior
  * state U, produced on the GPU with the boundary mapping the stage kernels use (no ghost ring is
  * stored by the solver itself).  Ug: host array of (ny+4)*(nx+4)*4 doubles. */
@@ -194,7 +215,10 @@ int fv_fp64_peak(double* dfma_per_second);
  * until exit), so grids are limited to FV_NOALLOC_MAX_CELLS cells (larger ones return FV_ERR_ARG).
  * All calls on a device share that scratch: calls that overlap on the GPU race and must be
  * serialised by the caller.  The first call on a device sets up the scratch address; make it before
- * any stream capture.  stream: a cudaStream_t or NULL.  No counterpart in the reference. */
+ * any stream capture, and do not use this entry point across cudaDeviceReset (the set-up is cached
+ * for the process).  d_U must be 16-byte aligned, as cudaMalloc'd memory is: the kernels move each
+ * cell with two 16-byte accesses, and a misaligned pointer returns FV_ERR_ARG with nothing launched.
+ * stream: a cudaStream_t or NULL.  No counterpart in the reference. */
 #define FV_NOALLOC_MAX_CELLS (128 * 128)
 int fv_step_noalloc(int nx, int ny, double x_min, double x_max, double y_min, double y_max, int bc_x, int bc_y,
                     int flux, int limiter, double* d_U, double dt, void* stream);

@@ -5,6 +5,6 @@ The directory name is not a Python identifier; import it with
 ``importlib.import_module("neural-pde-surrogate_b200")``.
 """
 from ._lib import FVError, NonPhysicalError, lib  # noqa: F401
-from .solver import BC, FLUXES, LIMITERS, Grid, Solver, eval_division, fill_ghosts, make_grid, riemann_flux  # noqa: F401
+from .solver import BC, FLUXES, LIMITERS, Grid, Solver, division_sweep, eval_division, fill_ghosts, make_grid, riemann_flux  # noqa: F401
 
-__all__ = ["BC", "FLUXES", "LIMITERS", "Grid", "Solver", "make_grid", "riemann_flux", "eval_division", "fill_ghosts", "FVError", "NonPhysicalError", "lib"]
+__all__ = ["BC", "FLUXES", "LIMITERS", "Grid", "Solver", "make_grid", "riemann_flux", "eval_division", "division_sweep", "fill_ghosts", "FVError", "NonPhysicalError", "lib"]

@@ -55,6 +55,8 @@ _PROTOS = {
     "fv_ensemble_get_stream": [_P, C.POINTER(C.c_void_p)],
     "fv_riemann_flux": [_I, _I, _I, _P, _P, _P],
     "fv_eval_division": [_I, _P, _P, _P],
+    "fv_eval_division_kind": [_I, _I, _P, _P, _P],
+    "fv_division_sweep": [_I, C.c_longlong, C.c_ulonglong, _LLP, _LLP],
     "fv_fill_ghosts": [_I, _I, _I, _I, _P, _P],
     "fv_profile": [_P, _I],
     "fv_profile_read": [_P, _DP, _DP, _LLP],

@@ -273,7 +273,8 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
     __syncthreads();
     FV_PHASE_MARK(2);
 
-    // P3: face fluxes, flux(to_conserved(edge(W_L, dW_L, +1)), to_conserved(edge(W_R, dW_R, -1)))
+    // P3: face fluxes, flux(to_conserved(edge(W_L, dW_L, +1)), to_conserved(edge(W_R, dW_R, -1))),
+    // with each side's to_primitive by face_side
     for (int e = threadIdx.x; e < NFX + NFY; e += NT) {
         Q4 wl, dl, wr, dr;
         const bool ydir = e >= NFX;
@@ -288,10 +289,13 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
             wl = lds(s.W, r + 1, k + 2); dl = lds(s.dY, r, k);
             wr = lds(s.W, r + 2, k + 2); dr = lds(s.dY, r + 1, k);
         }
-        Q4 UL = to_conserved(edge(wl, dl, +1.0));
-        Q4 UR = to_conserved(edge(wr, dr, -1.0));
-        if (ydir) { UL = swap_xy(UL); UR = swap_xy(UR); }
-        Q4 F = face_flux<FLUX>(UL, UR);
+        FaceSide L = face_side(edge(wl, dl, +1.0));
+        FaceSide R = face_side(edge(wr, dr, -1.0));
+        if (ydir) {
+            L.U = swap_xy(L.U); L.W = swap_xy(L.W);
+            R.U = swap_xy(R.U); R.W = swap_xy(R.W);
+        }
+        Q4 F = face_flux<FLUX>(L.U, L.W, R.U, R.W);
         if (ydir) sts(s.G, r, k, swap_xy(F));
         else sts(s.F, r, k, F);
     }

@@ -14,11 +14,17 @@
 // must be serialised by the caller.  The control block is cleared at the start of every call.
 // The first call on a device (that device current) looks up the array's device address with
 // cudaGetSymbolAddress and sets the kernels' shared-memory limit; make that first call before any
-// stream capture.
+// stream capture.  That set-up is cached for the life of the process: after cudaDeviceReset the
+// library's module may be reloaded at another address, so do not use this entry point across a
+// device reset.
+// The kernels move each cell with two 16-byte (double2) accesses, so d_U must be 16-byte aligned
+// (cudaMalloc'd memory is; a view at an odd double offset is not): a misaligned pointer is rejected
+// with FV_ERR_ARG before anything is launched.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <climits>
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/fv.h"
@@ -96,6 +102,8 @@ int setup(int dev, unsigned char** out) {
 extern "C" int fv_step_noalloc(int nx, int ny, double x_min, double x_max, double y_min, double y_max, int bc_x,
                                int bc_y, int flux, int limiter, double* d_U, double dt, void* stream) {
     if (!d_U) return fv_internal_set_error(FV_ERR_ARG, "fv_step_noalloc: d_U is NULL");
+    if (reinterpret_cast<uintptr_t>(d_U) & 15u)
+        return fv_internal_set_error(FV_ERR_ARG, "fv_step_noalloc: d_U must be 16-byte aligned");
     if (nx <= 0 || ny <= 0) return fv_internal_set_error(FV_ERR_ARG, "fv_step_noalloc: nx and ny must be positive");
     if ((long long)nx * ny > FV_NOALLOC_MAX_CELLS)
         return fv_internal_set_error(FV_ERR_ARG,

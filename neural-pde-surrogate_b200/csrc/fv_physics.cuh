@@ -71,10 +71,11 @@ __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 // y + y(1 - b y), q0 = a y, and Markstein's correction q0 + (a - q0 b) y (the method cited above).
 // Emulated on a CPU with seeds of relative error up to 2^-20 this gave the correctly rounded
 // quotient for all of 2e7 random operand pairs, and at most 1 ulp from 2^-14 seeds.  Operands
-// outside 2^-500 < |b| < 2^500, |a| < 2^500 (zeros, infinities, NaN, extremes) take `/`.
+// outside 2^-500 < |a|, |b| < 2^500 take `/`: zeros (so that a signed zero keeps IEEE's sign),
+// infinities, NaN, and the extremes whose quotient could be subnormal or overflow.
 __device__ __forceinline__ double fdiv(double a, double b) {
-    const double mb = fabs(b);
-    if (!(mb > 0x1p-500 && mb < 0x1p+500 && fabs(a) < 0x1p+500)) return a / b;
+    const double mb = fabs(b), ma = fabs(a);
+    if (!(mb > 0x1p-500 && mb < 0x1p+500 && ma > 0x1p-500 && ma < 0x1p+500)) return a / b;
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
     y = fma(y, fma(-b, y, 1.0), y);
@@ -92,6 +93,27 @@ __device__ __forceinline__ double div_z(double a, double b) {
     return fdiv(a, b);
 }
 
+// RN(m / rho) for m = RN(rho * u): the velocity to_primitive recovers from a momentum that
+// to_conserved formed from the same rho and u.  Every face state of the reference takes that round
+// trip (to_conserved(edge(...)) then to_primitive, solver2d.hpp:145-148,165-169 with
+// riemann2d.hpp:12,28), so the quotient can be decided without dividing.  e = rho*u - m is exact
+// (one fma: the error-free product of Dekker, and of Ogita, Rump and Oishi, SIAM J. Sci. Comput.
+// 26(6), 2005), so the exact quotient is m/rho = u - e/rho, and |e/rho| <= 2^-53 |u| (1 + 2^-53) <
+// ulp(u).  Its correctly rounded value is u when |e/rho| < ulp(u)/2, else the neighbour of u on the
+// side of -e/rho.  No tie can occur: the exact quotient of two doubles is never halfway between two
+// doubles.  When u is a power of two the product is exact and e = 0.  The bound 2^-300 < rho, |u| <
+// 2^300 keeps e, rho*ulp(u)/2 and rho*u normal; outside it (a zero, negative or extreme density, a
+// zero or extreme velocity) the division is done.
+__device__ __forceinline__ double div_back(double m, double rho, double u) {
+    const double au = fabs(u);
+    if (!(rho > 0x1p-300 && rho < 0x1p+300 && au > 0x1p-300 && au < 0x1p+300)) return div_z(m, rho);
+    const double e = fma(rho, u, -m);
+    const double half_ulp = __hiloint2double((__double2hiint(u) & 0x7ff00000) - (53 << 20), 0);  // 2^(k-53)
+    if (fabs(e) < rho * half_ulp) return u;
+    const long long bits = __double_as_longlong(u);
+    return __longlong_as_double(((e > 0.0) == (u > 0.0)) ? bits - 1 : bits + 1);  // toward zero if same sign
+}
+
 // state2d.hpp:16-19 (p / (GAMMA - 1.0) through div_gm1: same bits, fewer instructions)
 __device__ __forceinline__ Q4 to_conserved(const Q4& W) {
     return Q4{W.a, W.a * W.b, W.a * W.c, div_gm1(W.d) + 0.5 * W.a * (W.b * W.b + W.c * W.c)};
@@ -102,6 +124,24 @@ __device__ __forceinline__ Q4 to_primitive(const Q4& U) {
     double u = div_z(U.b, U.a), v = div_z(U.c, U.a);
     double p = GM1 * (U.d - 0.5 * U.a * (u * u + v * v));
     return Q4{U.a, u, v, p};
+}
+
+// One side of a face: U = to_conserved(We) of the MUSCL edge state We, and W = to_primitive(U), the
+// primitive state the reference's flux function recomputes from U (riemann2d.hpp:12,28).  The
+// velocities come from div_back (same bits as the divisions of to_primitive); the pressure is
+// to_primitive's expression on them.  The tolerance build keeps the edge state itself as W (within
+// an ulp per component of the round trip) and skips the recomputation.
+struct FaceSide {
+    Q4 U, W;
+};
+__device__ __forceinline__ FaceSide face_side(const Q4& We) {
+    const Q4 U = to_conserved(We);
+#ifndef FV_TOLERANCE_BUILD
+    const double u = div_back(U.b, We.a, We.b), v = div_back(U.c, We.a, We.c);
+    return FaceSide{U, Q4{U.a, u, v, GM1 * (U.d - 0.5 * U.a * (u * u + v * v))}};
+#else
+    return FaceSide{U, We};
+#endif
 }
 
 // state2d.hpp:27
@@ -142,9 +182,8 @@ __device__ __forceinline__ Q4 edge(const Q4& W, const Q4& dW, double s) {
     return Q4{W.a + h * dW.a, W.b + h * dW.b, W.c + h * dW.c, W.d + h * dW.d};
 }
 
-// riemann2d.hpp:11-15
-__device__ __forceinline__ Q4 rusanov_flux(const Q4& UL, const Q4& UR) {
-    Q4 WL = to_primitive(UL), WR = to_primitive(UR);
+// riemann2d.hpp:11-15, given WL = to_primitive(UL) and WR = to_primitive(UR)
+__device__ __forceinline__ Q4 rusanov_flux(const Q4& UL, const Q4& WL, const Q4& UR, const Q4& WR) {
     double s_max = smax(fabs(WL.b) + sound_speed(WL), fabs(WR.b) + sound_speed(WR));
     Q4 FL = flux_x(UL, WL), FR = flux_x(UR, WR);
     double h = 0.5 * s_max;
@@ -157,8 +196,7 @@ __device__ __forceinline__ Q4 rusanov_flux(const Q4& UL, const Q4& UR) {
 // (left when 0 <= SL or 0 <= S_star, as its first two branches are) and the star state is evaluated
 // once for that side, so that all lanes of a warp run one code path.  Every branch returns the same
 // expression on the same inputs as the reference, hence bit-identical results.
-__device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& UR) {
-    Q4 WL = to_primitive(UL), WR = to_primitive(UR);
+__device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& WL, const Q4& UR, const Q4& WR) {
     double aL = sound_speed(WL), aR = sound_speed(WR);
     double SL = smin(WL.b - aL, WR.b - aR);
     double SR = smax(WL.b + aL, WR.b + aR);
@@ -176,11 +214,17 @@ __device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& UR) {
     return Q4{F.a + S * (st.a - U.a), F.b + S * (st.b - U.b), F.c + S * (st.c - U.c), F.d + S * (st.d - U.d)};
 }
 
-// Flux scheme chosen at compile time (one kernel instance per scheme).
+// Flux scheme chosen at compile time (one kernel instance per scheme), on two face sides.
+template <int FLUX>
+__device__ __forceinline__ Q4 face_flux(const Q4& UL, const Q4& WL, const Q4& UR, const Q4& WR) {
+    if constexpr (FLUX == FLUX_HLLC) return hllc_flux(UL, WL, UR, WR);
+    else return rusanov_flux(UL, WL, UR, WR);
+}
+
+// The FluxFn interface itself (riemann2d.hpp:8): conserved states in, primitives recomputed.
 template <int FLUX>
 __device__ __forceinline__ Q4 face_flux(const Q4& UL, const Q4& UR) {
-    if constexpr (FLUX == FLUX_HLLC) return hllc_flux(UL, UR);
-    else return rusanov_flux(UL, UR);
+    return face_flux<FLUX>(UL, to_primitive(UL), UR, to_primitive(UR));
 }
 
 // state2d.hpp:39

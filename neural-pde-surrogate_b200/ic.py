@@ -115,6 +115,16 @@ def sample(family, index, n):
     return rho, u, v, p, t_end, {"family": family, "index": int(index), **params}
 
 
+def ensemble_spec(count=256, sizes=(64, 128, 256, 512), seed=2026):
+    """Members of the batched-ensemble workload: `count` periodic trajectories, alternately a
+    four-quadrant Riemann and a blast + bubble initial condition (member k is index k // 2 of its
+    family), each with a grid size drawn uniformly from `sizes` by a generator seeded with `seed`.
+    Returns a list of (family, index, n)."""
+    rng = np.random.default_rng(seed)
+    return [("riemann" if k % 2 == 0 else "blast", k // 2, int(sizes[int(rng.integers(len(sizes)))]))
+            for k in range(count)]
+
+
 def to_conserved(rho, u, v, p):
     """state2d.hpp:16-19 elementwise, same association (numpy rounds every operation separately,
     like the reference's build without FMA contraction).  Returns (ny, nx, 4)."""

@@ -220,17 +220,30 @@ def riemann_flux(flux, UL, UR, face="x"):
     return F
 
 
-def eval_division(a, b):
-    """a / b elementwise, computed on the GPU by the division the stage kernels use at every general
-    division site (fv_eval_division): IEEE in the parity build, the Newton-Raphson sequence in the
-    tolerance build."""
+DIVISIONS = {"general": 0, "gm1": 1, "zero": 2, "back": 3}  # FV_DIV_* of include/fv.h
+
+
+def eval_division(a, b, kind="general"):
+    """Elementwise quotients computed on the GPU by one of the stage kernels' division sequences
+    (fv_eval_division_kind): 'general' is a / b at every general division site (IEEE in the parity
+    build, the Newton-Raphson sequence in the tolerance build); 'gm1' is a / (GAMMA - 1) (b unused);
+    'zero' is a / b with the zero-numerator fast path; 'back' is RN(RN(a*b)/a), a face state's
+    velocity after the conserved/primitive round trip (a = rho, b = u)."""
     a = np.ascontiguousarray(a, np.float64)
-    b = np.ascontiguousarray(b, np.float64)
+    b = np.ascontiguousarray(np.zeros_like(a) if b is None else b, np.float64)
     if a.shape != b.shape:
         raise ValueError(f"a and b must have the same shape, got {a.shape} and {b.shape}")
     q = np.empty_like(a)
-    check(lib().fv_eval_division(a.size, _ptr(a), _ptr(b), _ptr(q)))
+    check(lib().fv_eval_division_kind(DIVISIONS[kind], a.size, _ptr(a), _ptr(b), _ptr(q)))
     return q
+
+
+def division_sweep(kind, n, seed=0):
+    """Draws n operand pairs on the GPU and counts the quotients of division sequence `kind` that
+    differ in any bit from IEEE division (fv_division_sweep).  Returns (mismatches, max ulps)."""
+    mism, ulps = C.c_longlong(), C.c_longlong()
+    check(lib().fv_division_sweep(DIVISIONS[kind], int(n), int(seed), C.byref(mism), C.byref(ulps)))
+    return mism.value, ulps.value
 
 
 def fill_ghosts(U, bc_x, bc_y):

@@ -1,6 +1,9 @@
 """Build recipe for the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
-  python oracle/build_oracle.py            # builds what it can
+  python oracle/build_oracle.py [--reference DIR]     # builds what it can
+
+DIR (or the environment variable FV_REFERENCE_SRC) is the reference's solver/src folder; the default
+is the read-only copy of the reference project this repository was built beside.
 
 1. oracle/libfvoracle.so  -- the plain-C restatement (oracle/fv_oracle.c), always built.
 2. oracle/_ref/libfvref.so -- oracle/ref_harness.cpp compiled against the reference's own solver
@@ -20,7 +23,7 @@ import tempfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference/solver/src")
+REF_SRC = Path(os.environ.get("FV_REFERENCE_SRC", "/root/reference/solver/src"))
 REF_OUT = HERE / "_ref"
 
 CFLAGS = ["-O3", "-fopenmp", "-ffp-contract=off", "-fPIC"]
@@ -88,5 +91,7 @@ def build(force=False):
 
 
 if __name__ == "__main__":
+    if "--reference" in sys.argv:
+        REF_SRC = Path(sys.argv[sys.argv.index("--reference") + 1])
     build(force="--force" in sys.argv)
     print("oracle built:", HERE / "libfvoracle.so", "| reference:", REF_OUT / "libfvref.so")

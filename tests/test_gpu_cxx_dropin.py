@@ -1,8 +1,7 @@
 """GPU run of the reference's own test_solver2d.cpp, built unmodified against libfv through the C++
-drop-in Solver header (oracle/_ref/test_solver2d_fv, made by oracle/build_oracle.py).
-
-Staged: pytest collects only test_*.py, so this runs once the file is renamed to
-test_gpu_cxx_dropin.py, after it has passed on a B200.
+drop-in Solver header (oracle/_ref/test_solver2d_fv, made by oracle/build_oracle.py).  The program's
+ten checks (free stream, x/y transpose symmetry, conservation, the Sod plateaus; test_solver2d.cpp:37-108)
+must all pass with every step running on the GPU.
 """
 import subprocess
 from pathlib import Path

@@ -62,3 +62,37 @@ def test_noalloc_rejects_grids_beyond_the_limit(cuda_ok):
     rc = _noalloc()(MAX_CELLS + 1, 1, 0.0, 1.0, 0.0, 1.0, 1, 1, 1, 3, C.c_void_p(d_U.data_ptr()), 1e-3, None)
     assert rc == 1
     assert b"FV_NOALLOC_MAX_CELLS" in fv.lib().fv_last_error()
+
+
+def _rejects(args, needle):
+    """Calls the entry point on a 64 x 64 state with one argument replaced (`offset`: bytes added to
+    the state's address, inside the buffer, which has two spare doubles) and checks it is refused."""
+    import torch
+    d_U = torch.zeros(64 * 64 * 4 + 2, dtype=torch.float64, device="cuda")
+    a = dict(nx=64, ny=64, x0=0.0, x1=1.0, y0=0.0, y1=1.0, bcx=1, bcy=1, flux=1, lim=3, offset=0, null=False,
+             dt=1e-3)
+    a.update(args)
+    ptr = None if a["null"] else C.c_void_p(d_U.data_ptr() + a["offset"])
+    before = d_U.clone()
+    rc = _noalloc()(a["nx"], a["ny"], a["x0"], a["x1"], a["y0"], a["y1"], a["bcx"], a["bcy"], a["flux"], a["lim"],
+                    ptr, a["dt"], None)
+    torch.cuda.synchronize()
+    assert rc == 1, rc
+    assert needle in fv.lib().fv_last_error()
+    assert torch.equal(before, d_U)  # rejected before any kernel ran
+
+
+@pytest.mark.parametrize("args,needle", [
+    (dict(flux=7), b"unknown flux/limiter/bc"), (dict(lim=-1), b"unknown flux/limiter/bc"),
+    (dict(lim=4), b"unknown flux/limiter/bc"), (dict(bcx=2), b"unknown flux/limiter/bc"),
+    (dict(bcy=-1), b"unknown flux/limiter/bc"), (dict(x1=0.0), b"empty domain"), (dict(y0=2.0), b"empty domain"),
+    (dict(nx=0), b"must be positive"), (dict(ny=-3), b"must be positive"), (dict(null=True), b"NULL"),
+])
+def test_noalloc_rejects_invalid_arguments(cuda_ok, args, needle):
+    _rejects(args, needle)
+
+
+def test_noalloc_rejects_a_misaligned_state(cuda_ok):
+    """A state 8 bytes off a 16-byte boundary (a view at an odd double offset) is refused with
+    FV_ERR_ARG, not handed to kernels that load each cell as two 16-byte words."""
+    _rejects(dict(offset=8), b"16-byte aligned")
