@@ -195,6 +195,16 @@ int fv_tile_variant(int variant, int* tx, int* ty, int* threads);
  * duration in ms of stage-1 and stage-2 launches and the number of steps timed since enabling. */
 int fv_profile(fv_solver* s, int enable);
 int fv_profile_read(fv_solver* s, double* ms_stage1, double* ms_stage2, long long* steps_timed);
+/* The same, per whole step and for both kernel paths: fv_advance_to runs on the persistent stepper
+ * (one cooperative launch per batch of steps, FV_STEPPER=0 in the environment to use the per-stage
+ * kernels instead), whose stages have no launches of their own.  ms_per_step: mean device time per
+ * step of every timed launch since fv_profile(s, 1); steps: steps timed; launches: stepper launches
+ * timed.  Any pointer may be NULL. */
+int fv_profile_steps(fv_solver* s, double* ms_per_step, long long* steps, long long* launches);
+/* The tile shape the handle's persistent stepper uses (0s before its first fv_advance_to, or when the
+ * stepper is switched off).  Chosen like the per-stage kernels' shape, by timing each on a copy of
+ * the state; FV_STEPPER_TILE=<index> fixes it. */
+int fv_stepper_tile(fv_solver* s, int* tx, int* ty, int* threads);
 
 /* Self-test of the library's bounded waits: runs the wait used for every TMA copy and tensor-core
  * batch on a barrier that nothing arrives at, with a 10 ms limit.  Returns FV_ERR_TIMEOUT when the

@@ -60,6 +60,8 @@ _PROTOS = {
     "fv_fill_ghosts": [_I, _I, _I, _I, _P, _P],
     "fv_profile": [_P, _I],
     "fv_profile_read": [_P, _DP, _DP, _LLP],
+    "fv_profile_steps": [_P, _DP, _LLP, _LLP],
+    "fv_stepper_tile": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
     "fv_launch_count": [_P, _LLP],
     "fv_fp64_peak": [_DP],
     "fv_wait_selftest": [],

@@ -24,7 +24,7 @@ LIBS = {
     "libfv.so": {
         "sources": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_ensemble.cu", "fvnet_conv.cu", "fvnet_ops.cu",
                     "fv_selftest.cu"],
-        "deps": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_selftest.cu", "fv_ensemble.cu", "fv_kernels.cuh", "fv_physics.cuh",
+        "deps": ["fv_api.cu", "fv_peak.cu", "fv_noalloc.cu", "fv_selftest.cu", "fv_ensemble.cu", "fv_kernels.cuh", "fv_physics.cuh", "fv_stepper.cuh",
                  "fvnet_conv.cu", "fvnet_ops.cu", "tc_sm100.cuh"],
         "flags": ["--fmad=false"],
         "headers": ["fv.h", "fvnet.h"],

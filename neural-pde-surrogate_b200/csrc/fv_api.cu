@@ -11,12 +11,14 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <tuple>
 #include <vector>
 
 #include "../../include/fv.h"
 #include "fv_kernels.cuh"
+#include "fv_stepper.cuh"
 
 using namespace fv;
 
@@ -87,9 +89,87 @@ const std::vector<TileVariant>& variants() {
     return v;
 }
 
+// Tile shapes the persistent stepper (fv_stepper.cuh) is instantiated for; `variant` is the index of
+// the same shape in variants() (whose TMA descriptors it shares).  All give bit-identical results.
+using StepperFn = void (*)(GridDesc, TileMaps, StepperTiles);
+struct StepperVariant {
+    int variant;
+    int tx, ty, nt;
+    size_t smem;
+    StepperFn fn[2][4];  // [flux][limiter]
+};
+
+template <int TX, int TY, int NT, int MINB>
+struct StepperMaker {
+    template <int F, int L>
+    static void one(StepperVariant& v) { v.fn[F][L] = stepper_kernel<F, L, TX, TY, NT, MINB>; }
+    static StepperVariant make(int variant) {
+        StepperVariant v{variant, TX, TY, NT, sizeof(TileSmem<TX, TY>), {}};
+        one<0, 0>(v); one<0, 1>(v); one<0, 2>(v); one<0, 3>(v);
+        one<1, 0>(v); one<1, 1>(v); one<1, 2>(v); one<1, 3>(v);
+        return v;
+    }
+};
+
+const std::vector<StepperVariant>& stepper_variants() {
+    static const std::vector<StepperVariant> v = {
+        StepperMaker<16, 14, 256, 4>::make(6),  // 0: default
+        StepperMaker<16, 16, 256, 4>::make(2),  // 1
+        StepperMaker<32, 8, 256, 4>::make(0),   // 2
+        StepperMaker<16, 7, 128, 8>::make(8),   // 3
+        StepperMaker<32, 16, 512, 2>::make(1),  // 4
+    };
+    return v;
+}
+
 // Autotuned choice per (device, nx, ny, flux, limiter), shared by all handles of the process.
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned_stepper;
+
+// Host copy of bc_index (fv_physics.cuh) for the stepper's dependency lists.
+int host_bc_index(int g, int n, int bc) {
+    if (bc == BC_PERIODIC) {
+        const int m = g % n;
+        return m < 0 ? m + n : m;
+    }
+    return g < 0 ? 0 : (g >= n ? n - 1 : g);
+}
+
+// The stepper's dependency list of every tile: the tiles that hold a cell of its halo box
+// [i0 - 2, i0 + tx + 1] x [j0 - 2, j0 + ty + 1] once mapped through the boundary conditions (whose
+// stage outputs it reads), and the tiles whose halo box holds one of its cells (which read what it
+// overwrites), itself included.  Compressed rows: off has ntx*nty + 1 entries.
+void build_stepper_deps(int nx, int ny, int bc_x, int bc_y, int tx, int ty, std::vector<int>& off,
+                        std::vector<int>& idx) {
+    const int ntx = (nx + tx - 1) / tx, nty = (ny + ty - 1) / ty, T = ntx * nty;
+    auto axis = [](int t, int w, int n, int bc) {
+        std::set<int> out;
+        for (int c = t * w - 2; c <= t * w + w + 1; ++c) out.insert(host_bc_index(c, n, bc) / w);
+        return out;
+    };
+    std::vector<std::set<int>> deps(T);
+    for (int b = 0; b < nty; ++b) {
+        const std::set<int> ys = axis(b, ty, ny, bc_y);
+        for (int a = 0; a < ntx; ++a) {
+            const std::set<int> xs = axis(a, tx, nx, bc_x);
+            const int t = b * ntx + a;
+            for (int y : ys)
+                for (int x : xs) {
+                    const int d = y * ntx + x;
+                    deps[t].insert(d);  // t reads d
+                    deps[d].insert(t);  // d overwrites what t reads
+                }
+        }
+    }
+    off.assign(1, 0);
+    idx.clear();
+    for (int t = 0; t < T; ++t) {
+        deps[t].insert(t);
+        idx.insert(idx.end(), deps[t].begin(), deps[t].end());
+        off.push_back((int)idx.size());
+    }
+}
 
 }  // namespace
 
@@ -123,6 +203,19 @@ struct fv_solver {
     int ring_head = 0, ring_used = 0;
     double ms1 = 0.0, ms2 = 0.0;
     long long timed = 0;
+    // persistent stepper: tile shape (index into stepper_variants(), -1 before the first choice), its
+    // TMA descriptors, flags and dependency lists (one device allocation), and its timing
+    int svariant = -1;
+    bool stuned = false;
+    TileMaps smaps{};
+    int smaps_variant = -1;
+    void* sbuf = nullptr;
+    int sbuf_variant = -1;
+    StepperTiles st{};
+    int sgrid = 0;          // co-resident CTAs of the chosen stepper kernel
+    cudaEvent_t sev[2] = {};
+    double step_ms = 0.0;   // stepper launches' device time since fv_profile(1) (all kernels of a launch)
+    long long step_steps = 0, step_launches = 0;
 
     size_t ncell() const { return size_t(nx) * ny; }
     GridDesc desc() const {
@@ -355,6 +448,212 @@ int autotune(fv_solver* s, int steps, int* chosen) {
     return FV_OK;
 }
 
+// ---- persistent stepper (fv_stepper.cuh) --------------------------------------------------------
+
+// FV_STEPPER=0 in the environment keeps fv_advance_to on the per-stage kernels (for comparisons).
+bool stepper_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("FV_STEPPER");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
+// Readies stepper shape sv for the handle: kernel attributes and co-residency (cached per kernel),
+// the flags and dependency lists of the handle's grid (one device allocation, rebuilt when the shape
+// changes) and the TMA descriptors of the shape.
+int prepare_stepper(fv_solver* s, int sv) {
+    const StepperVariant& v = stepper_variants()[sv];
+    StepperFn fn = v.fn[s->flux][s->lim];
+    static std::mutex mu;
+    static std::map<std::pair<int, StepperFn>, int> resident;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = resident.find({s->device, fn});
+        if (it == resident.end()) {
+            FV_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem));
+            FV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, v.nt, v.smem));
+            resident[{s->device, fn}] = per_sm;
+        } else {
+            per_sm = it->second;
+        }
+    }
+    int sms = 0;
+    FV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    if (per_sm < 1) return set_error(FV_ERR_CUDA, "stepper tile %dx%d cannot be resident", v.tx, v.ty);
+    if (s->sbuf_variant != sv) {
+        std::vector<int> off, idx;
+        build_stepper_deps(s->nx, s->ny, s->bc_x, s->bc_y, v.tx, v.ty, off, idx);
+        const size_t T = off.size() - 1;
+        cudaFree(s->sbuf);
+        s->sbuf = nullptr;
+        s->sbuf_variant = -1;
+        FV_CUDA(cudaMalloc(&s->sbuf, 2 * T * sizeof(unsigned) + (off.size() + idx.size()) * sizeof(int)));
+        unsigned* flags = static_cast<unsigned*>(s->sbuf);
+        int* doff = reinterpret_cast<int*>(flags + 2 * T);
+        int* didx = doff + off.size();
+        FV_CUDA(cudaMemcpyAsync(doff, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+        FV_CUDA(cudaMemcpyAsync(didx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+        FV_CUDA(cudaStreamSynchronize(s->stream));  // the host vectors go out of scope
+        s->st = StepperTiles{flags, flags + T, doff, didx, (s->nx + v.tx - 1) / v.tx, (s->ny + v.ty - 1) / v.ty};
+        s->sbuf_variant = sv;
+    }
+    if (s->smaps_variant != v.variant) {
+        int rc = encode_maps(s->desc(), v.tx, v.ty, &s->smaps);
+        if (rc) return rc;
+        s->smaps_variant = v.variant;
+    }
+    s->sgrid = per_sm * sms;
+    return FV_OK;
+}
+
+// One stepper launch on grid g: the prologue kernel (queue, flags, publication of the current step)
+// and the cooperative kernel, which runs at most nsteps steps and stops by itself where the loop
+// reaches t_next, a bad cell appears, or a bounded wait runs out.
+int enqueue_stepper(const GridDesc& g, const TileMaps& tm, const StepperTiles& st, int sv, int flux, int lim,
+                    int grid, long long nsteps, cudaStream_t stream) {
+    const StepperVariant& v = stepper_variants()[sv];
+    const long long T = (long long)st.ntx * st.nty;
+    stepper_begin_kernel<<<(unsigned)std::max<long long>(1, std::min<long long>((T + 255) / 256, 148)), 256, 0, stream>>>(
+        g, st, nsteps);
+    FV_CUDA(cudaGetLastError());
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: an item's waits always end
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)std::min<long long>(grid, 2 * T * nsteps));
+    cfg.blockDim = dim3(v.nt);
+    cfg.dynamicSmemBytes = v.smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FV_CUDA(cudaLaunchKernelEx(&cfg, v.fn[flux][lim], g, tm, st));
+    return FV_OK;
+}
+
+// Times every stepper shape for `steps` fixed-dt steps on copies of the current state (the handle's
+// state, time and control block are untouched) and keeps the fastest: the persistent counterpart of
+// autotune().  FV_STEPPER_TILE=<index> fixes the shape instead.
+int autotune_stepper(fv_solver* s, int steps) {
+    s->stuned = true;
+    s->svariant = 0;
+    const auto key = std::make_tuple(s->device, s->nx, s->ny, s->flux, s->lim);
+    const char* env = getenv("FV_STEPPER_TILE");
+    if (env && atoi(env) >= 0 && atoi(env) < (int)stepper_variants().size()) {
+        s->svariant = atoi(env);
+        return FV_OK;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned_stepper.find(key);
+        if (it != g_tuned_stepper.end()) {
+            s->svariant = it->second;
+            return FV_OK;
+        }
+    }
+    if (!s->has_state) return FV_OK;
+    double dt = 1e-6;
+    int rc = read_ctrl(s);
+    if (rc) return rc;
+    {
+        const FvCtrl& c = *s->h_ctrl;
+        double sx, sy;
+        std::memcpy(&sx, &c.sxy[c.step & 1][0], 8);
+        std::memcpy(&sy, &c.sxy[c.step & 1][1], 8);
+        const double d = s->cfl / (sx / s->dx + sy / s->dy);
+        if (d > 0.0 && std::isfinite(d)) dt = d;
+    }
+    const size_t n = s->ncell(), bytes = n * sizeof(Q4);
+    Q4* tmp = nullptr;
+    FvCtrl* ct = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int best = 0;
+    float best_ms = 1e30f;
+    cudaError_t e = cudaMalloc(&tmp, 4 * bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&ct, sizeof(FvCtrl));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    for (int v = 0; e == cudaSuccess && rc == FV_OK && v < (int)stepper_variants().size(); ++v) {
+        if ((rc = prepare_stepper(s, v))) break;
+        GridDesc g = s->desc();
+        g.U = tmp; g.U1 = tmp + n; g.W = tmp + 2 * n; g.W1 = tmp + 3 * n; g.ctrl = ct;
+        TileMaps tm;
+        if ((rc = encode_maps(g, stepper_variants()[v].tx, stepper_variants()[v].ty, &tm))) break;
+        float ms = 0.f;
+        for (int pass = 0; pass < 2 && rc == FV_OK && e == cudaSuccess; ++pass) {  // pass 0 warms up
+            e = cudaMemcpyAsync(g.U, s->U, bytes, cudaMemcpyDeviceToDevice, s->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(g.W, s->W, bytes, cudaMemcpyDeviceToDevice, s->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(ct, s->ctrl, sizeof(FvCtrl), cudaMemcpyDeviceToDevice, s->stream);
+            if (e != cudaSuccess) break;
+            ctrl_set_kernel<<<1, 1, 0, s->stream>>>(ct, MODE_FIXED, 0.0, dt);
+            ctrl_reset_kernel<<<1, 1, 0, s->stream>>>(ct, 0.0, 1);  // clears any status of the copy
+            if ((e = cudaEventRecord(e0, s->stream)) != cudaSuccess) break;
+            rc = enqueue_stepper(g, tm, s->st, v, s->flux, s->lim, s->sgrid, pass ? steps : 2, s->stream);
+            if (rc) break;
+            if ((e = cudaEventRecord(e1, s->stream)) != cudaSuccess) break;
+            if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            if ((e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
+            s->launches += 4;
+        }
+        if (rc == FV_OK && e == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(tmp);
+    cudaFree(ct);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(FV_ERR_CUDA, "stepper autotune: %s", cudaGetErrorString(e));
+    s->svariant = best;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned_stepper[key] = best;
+    return FV_OK;
+}
+
+// fv_advance_to on the persistent stepper: one launch per batch of up to 4096 steps (the kernel
+// stops by itself at t_next), the control block read once per launch.  The control block has been
+// set to loop mode and read into h_ctrl by the caller.
+int advance_stepper(fv_solver* s, double t_next) {
+    if (!s->stuned) {
+        int rc = autotune_stepper(s, 8);
+        if (rc) return rc;
+    }
+    int rc = prepare_stepper(s, s->svariant);
+    if (rc) return rc;
+    for (;;) {
+        const FvCtrl& c = *s->h_ctrl;
+        if (c.status) break;
+        const double t = c.t[c.step & 1];
+        if (!(t < t_next)) break;
+        double sx, sy;
+        std::memcpy(&sx, &c.sxy[c.step & 1][0], 8);
+        std::memcpy(&sy, &c.sxy[c.step & 1][1], 8);
+        const double dt_est = s->cfl / (sx / s->dx + sy / s->dy);
+        const double est = (dt_est > 0.0) ? std::ceil((t_next - t) / dt_est) : 1.0;
+        const long long nsteps = (long long)std::min(4096.0, std::max(1.0, 2.0 * est + 16.0));
+        const long long before = c.step;
+        if (s->profiling) FV_CUDA(cudaEventRecord(s->sev[0], s->stream));
+        if ((rc = enqueue_stepper(s->desc(), s->smaps, s->st, s->svariant, s->flux, s->lim, s->sgrid, nsteps,
+                                  s->stream)))
+            return rc;
+        s->launches += 2;
+        if (s->profiling) FV_CUDA(cudaEventRecord(s->sev[1], s->stream));
+        if ((rc = read_ctrl(s))) return rc;
+        if (s->profiling) {
+            float ms = 0.f;
+            FV_CUDA(cudaEventElapsedTime(&ms, s->sev[0], s->sev[1]));
+            s->step_ms += ms;
+            s->step_steps += s->h_ctrl->step - before;
+            s->step_launches++;
+        }
+        if (s->h_ctrl->step == before) break;  // nothing ran (the control block stopped the grid)
+    }
+    return FV_OK;
+}
+
 bool valid_common(int flux, int lim, int bc_x, int bc_y) {
     return (flux == FLUX_HLLC || flux == FLUX_RUSANOV) && lim >= LIM_NONE && lim <= LIM_VANLEER &&
            (bc_x == BC_PERIODIC || bc_x == BC_TRANSMISSIVE) && (bc_y == BC_PERIODIC || bc_y == BC_TRANSMISSIVE);
@@ -446,6 +745,9 @@ int fv_destroy(fv_solver* s) {
     for (auto& tri : s->ev)
         for (cudaEvent_t& e : tri)
             if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : s->sev)
+        if (e) cudaEventDestroy(e);
+    cudaFree(s->sbuf);
     cudaFree(s->U);
     cudaFree(s->U1);
     cudaFree(s->W);
@@ -559,8 +861,12 @@ int fv_advance_to(fv_solver* s, double t_next, double* t_out, long long* steps_o
     FV_CUDA(cudaGetLastError());
     int rc = read_ctrl(s);
     if (rc) return rc;
-    // Steps are queued in batches sized from the last dt; steps queued after t reaches t_next (or
-    // after a non-physical state) exit at their first instruction, so a batch may overshoot freely.
+    if (stepper_enabled()) {
+        if ((rc = advance_stepper(s, t_next))) return rc;
+    }
+    // Per-stage kernels: steps are queued in batches sized from the last dt; steps queued after t
+    // reaches t_next (or after a non-physical state) exit at their first instruction, so a batch may
+    // overshoot freely.
     const int kMaxBatch = 256;
     for (;;) {
         const FvCtrl& c = *s->h_ctrl;
@@ -587,7 +893,9 @@ int fv_advance_to(fv_solver* s, double t_next, double* t_out, long long* steps_o
         return set_error(FV_ERR_NONPHYSICAL, "Non-physical state in cell (%d, %d)", c.bad_index % s->nx,
                          c.bad_index / s->nx);
     }
-    if (c.status == FV_ERR_TIMEOUT) return set_error(FV_ERR_TIMEOUT, "fv_advance_to: a tile's TMA load did not land");
+    if (c.status == FV_ERR_TIMEOUT)
+        return set_error(FV_ERR_TIMEOUT, "fv_advance_to: a bounded device wait ran out (a tile's TMA load or a "
+                                         "stepper dependency)");
     return FV_OK;
 }
 
@@ -766,6 +1074,7 @@ int fv_profile(fv_solver* s, int enable) {
     if (enable && !s->ev[0][0]) {
         for (auto& tri : s->ev)
             for (cudaEvent_t& e : tri) FV_CUDA(cudaEventCreate(&e));
+        for (cudaEvent_t& e : s->sev) FV_CUDA(cudaEventCreate(&e));
     }
     while (s->ring_used) {
         int rc = retire_oldest(s);
@@ -774,6 +1083,37 @@ int fv_profile(fv_solver* s, int enable) {
     s->profiling = enable != 0;
     s->ms1 = s->ms2 = 0.0;
     s->timed = 0;
+    s->step_ms = 0.0;
+    s->step_steps = s->step_launches = 0;
+    return FV_OK;
+}
+
+int fv_profile_steps(fv_solver* s, double* ms_per_step, long long* steps, long long* launches) {
+    if (!s) return set_error(FV_ERR_ARG, "fv_profile_steps: NULL handle");
+    while (s->ring_used) {
+        int rc = retire_oldest(s);
+        if (rc) return rc;
+    }
+    const long long n = s->step_steps + s->timed;
+    const double ms = s->step_ms + s->ms1 + s->ms2;  // ms1, ms2: totals over the timed per-stage steps
+    if (ms_per_step) *ms_per_step = n ? ms / n : 0.0;
+    if (steps) *steps = n;
+    if (launches) *launches = s->step_launches;
+    return FV_OK;
+}
+
+int fv_stepper_tile(fv_solver* s, int* tx, int* ty, int* threads) {
+    if (!s) return set_error(FV_ERR_ARG, "fv_stepper_tile: NULL handle");
+    if (!stepper_enabled() || s->svariant < 0) {
+        if (tx) *tx = 0;
+        if (ty) *ty = 0;
+        if (threads) *threads = 0;
+        return FV_OK;
+    }
+    const StepperVariant& v = stepper_variants()[s->svariant];
+    if (tx) *tx = v.tx;
+    if (ty) *ty = v.ty;
+    if (threads) *threads = v.nt;
     return FV_OK;
 }
 

@@ -76,6 +76,15 @@ struct FvCtrl {
     int status;                    // 0, FV_ERR_NONPHYSICAL, or FV_ERR_TIMEOUT (a bounded wait ran out)
     int bad_index;                 // row-major index recorded with status
     int pad_;
+    // persistent stepper (fv_stepper.cuh), one launch at a time: its work queue, and what each
+    // completed step publishes for the next (step s's dt in sdt[s & 1], whether it runs in srun[s & 1])
+    unsigned long long queue;      // next work item of the launch
+    unsigned long long done2;      // stage-2 items completed in the launch
+    long long complete;            // last step whose stage 2 has finished on every tile
+    long long stop;                // first step that does not run (LLONG_MAX while unknown)
+    long long s0, s_end;           // first step of the launch; steps < s_end may run
+    double sdt[2];
+    int srun[2];
 };
 
 // One grid as the stage kernels see it.  W and W1 hold to_primitive(U) and to_primitive(U1): each
@@ -107,6 +116,19 @@ __device__ __forceinline__ Q4 ldg_w(const Q4* W, size_t n, size_t k) {
     const double2* p = reinterpret_cast<const double2*>(W);
     const double2 lo = __ldg(p + k), hi = __ldg(p + n + k);
     return Q4{lo.x, lo.y, hi.x, hi.y};
+}
+// The same loads through L2 only (ld.global.cg), for data that other CTAs of the same launch wrote:
+// the persistent stepper reads fields its own launch produced, which a non-coherent (__ldg) or
+// L1-cached load could see stale.
+__device__ __forceinline__ Q4 ldcg_w(const Q4* W, size_t n, size_t k) {
+    const double2* p = reinterpret_cast<const double2*>(W);
+    const double2 lo = __ldcg(p + k), hi = __ldcg(p + n + k);
+    return Q4{lo.x, lo.y, hi.x, hi.y};
+}
+__device__ __forceinline__ Q4 ldcg_q4(const Q4* p) {
+    const double2* v = reinterpret_cast<const double2*>(p);
+    const double2 x = __ldcg(v), y = __ldcg(v + 1);
+    return Q4{x.x, x.y, y.x, y.y};
 }
 __device__ __forceinline__ void st_w(Q4* W, size_t n, size_t k, const Q4& q) {
     double2* p = reinterpret_cast<double2*>(W);
@@ -214,10 +236,19 @@ __device__ __forceinline__ bool stage1_control(FvCtrl* c, const GridDesc& g, boo
 // tm: the grid's TMA descriptors for this tile shape, or nullptr; s.bar must have been initialised
 // (count 1) by the caller, and `phase` is the barrier's next phase parity (flipped after every TMA
 // tile; CTA-uniform).
-template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, class Ctl>
+// Two hooks serve the persistent stepper (fv_stepper.cuh); the per-stage kernels use their defaults:
+//  pre4()   -- called by every thread between P3 and P4 (dt is first read in P4); returning false
+//              leaves the tile without writing anything (the stepper waits there for the step's dt).
+//  COHERENT -- global loads of the stage inputs through L2 (ld.global.cg) instead of the
+//              non-coherent / L1 paths, for inputs written earlier in the same launch.
+struct NoPre4 {
+    __device__ __forceinline__ bool operator()() const { return true; }
+};
+
+template <int FLUX, int LIM, int STAGE, int TX, int TY, int NT, class Ctl, class Pre4 = NoPre4, bool COHERENT = false>
 __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm, uint32_t& phase, int i0, int j0,
                                           const double& dt, const int& go, Ctl ctl, TileSmem<TX, TY>& s, double& sx,
-                                          double& sy, int& bad) {
+                                          double& sy, int& bad, Pre4 pre4 = Pre4()) {
     using S = TileSmem<TX, TY>;
     constexpr int HX = S::HX, HY = S::HY;
     constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
@@ -243,7 +274,8 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
             const int r = e / HX, col = e - r * HX;
             const int gi = bc_index(i0 - 2 + col, nx, g.bc_x);
             const int gj = bc_index(j0 - 2 + r, ny, g.bc_y);
-            sts(s.W, r, col, ldg_w(Win, ncell, (size_t)gj * nx + gi));
+            const size_t k = (size_t)gj * nx + gi;
+            sts(s.W, r, col, COHERENT ? ldcg_w(Win, ncell, k) : ldg_w(Win, ncell, k));
         }
     }
     ctl();
@@ -301,6 +333,7 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
     }
     __syncthreads();
     FV_PHASE_MARK(3);
+    if (!pre4()) return false;
 
     // P4: divergence + stage update
     const double cx = g.cx, cy = g.cy;
@@ -321,13 +354,13 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
         L.d = L.d + cy * Gb.d; L.d = L.d - cy * Gt.d;
         const size_t idx = (size_t)j * nx + i;
         if constexpr (STAGE == 1) {
-            const Q4 u = ldg_q4(g.U + idx);
+            const Q4 u = COHERENT ? ldcg_q4(g.U + idx) : ldg_q4(g.U + idx);
             const Q4 u1{u.a + dt * L.a, u.b + dt * L.b, u.c + dt * L.c, u.d + dt * L.d};
             st_q4(g.U1 + idx, u1);
             st_w(g.W1, ncell, idx, to_primitive(u1));
         } else {
-            const Q4 u = ld_q4(g.U + idx);
-            const Q4 u1 = ldg_q4(g.U1 + idx);
+            const Q4 u = COHERENT ? ldcg_q4(g.U + idx) : ld_q4(g.U + idx);
+            const Q4 u1 = COHERENT ? ldcg_q4(g.U1 + idx) : ldg_q4(g.U1 + idx);
             const Q4 un{0.5 * (u.a + u1.a + dt * L.a), 0.5 * (u.b + u1.b + dt * L.b),
                         0.5 * (u.c + u1.c + dt * L.c), 0.5 * (u.d + u1.d + dt * L.d)};
             const Q4 wn = to_primitive(un);

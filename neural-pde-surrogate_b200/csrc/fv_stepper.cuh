@@ -1,0 +1,282 @@
+// Persistent dataflow stepper: one cooperative launch advances one grid by many SSP-RK2 steps.
+//
+// The per-stage kernels (fv_kernels.cuh) launch twice per step, and every launch drains: the last
+// tiles of a stage finish at different times while the SMs that finished first sit idle, and the
+// next stage starts only when the whole grid is done.  Here a grid of (SMs x resident CTAs) CTAs
+// stays resident and pulls work items from one queue in a fixed order:
+//     item k  ->  step s = s0 + k / (2T), stage 1 if k mod 2T < T else stage 2, tile k mod T
+// (T tiles).  An item waits only for what it reads or overwrites, never for the whole grid:
+//   * stage 1 of (s, t) reads U^s, W^s of t and its halo and overwrites U1, W1 of t, which stage 2
+//     of step s-1 read: it waits until stage 2 of step s-1 has finished on t's neighbours
+//     (flag2[n] >= s for every n in the tile's dependency list: the tiles its halo box maps to,
+//     through the boundary conditions, and the tiles whose halo box maps to it);
+//   * stage 2 of (s, t) likewise waits for stage 1 of step s on the neighbours (flag1[n] >= s + 1);
+//   * the time step is global: dt_s = min(cfl / (sx/dx + sy/dy), t_next - t_s) needs the wave speeds
+//     of all of U^s (solver2d.hpp:67-83, main2d.cpp:238).  Stage 1 therefore computes its slopes and
+//     face fluxes (phases P1-P3, the bulk of the work) first and waits for the step to be published
+//     only before its update (P4); stage 2 waits before it starts.  The last stage-2 item of step s
+//     publishes step s + 1 (publish_step), so the next step's first tiles overlap the current step's
+//     last ones instead of waiting for a drained grid.
+// Items wait only on items earlier in the queue, all CTAs are co-resident (cooperative launch), so
+// every wait ends; each is bounded in time all the same (FV_ERR_TIMEOUT, no hang).  The arithmetic
+// is tile_body's, so results are bit-identical to the per-stage kernels and to the reference.
+//
+// Memory ordering: a finished item's stores are published by one release store of its flag after
+// a CTA barrier (cumulative at GPU scope); a waiting item acquires the flags, then its CTA barrier
+// orders every thread's loads after them.  Fields written in the same launch are read through L2
+// (tile_body's COHERENT loads) or by TMA, after a proxy fence.
+#pragma once
+#include "fv_kernels.cuh"
+
+namespace fv {
+
+__device__ __forceinline__ long long ld_acquire(const long long* p) {
+    long long v;
+    asm volatile("ld.acquire.gpu.global.s64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(long long* p, long long v) {
+    asm volatile("st.release.gpu.global.s64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Orders this thread's generic-proxy view of global memory with its asynchronous-proxy (TMA)
+// accesses: W and W1 are written by ordinary stores and read by TMA in the same launch.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// Tiles of the stepper's grid and their dependency lists (compressed rows: the dependencies of tile
+// t are dep_idx[dep_off[t] .. dep_off[t+1]), built on the host by build_stepper_deps).
+struct StepperTiles {
+    unsigned* flag1;       // per tile: number of steps whose stage 1 has finished on it
+    unsigned* flag2;       // per tile: number of steps whose stage 2 has finished on it
+    const int* dep_off;
+    const int* dep_idx;
+    int ntx, nty;
+};
+
+constexpr unsigned long long kStepperWaitNs = 1000000000ull;  // 1 s: far above any legitimate wait
+
+__device__ __forceinline__ int status_now(const FvCtrl* c) { return __ldcg(&c->status); }
+
+// Lane 0 waits until step `target` has been published (c->complete >= target).  Returns false when
+// it never will be -- an earlier step does not run (c->stop <= target: t_next reached, a bad cell, or
+// the launch's last step) -- on a timeout (recorded as FV_ERR_TIMEOUT), or when another CTA has
+// stopped the grid.
+__device__ __forceinline__ bool wait_complete(FvCtrl* c, long long target) {
+    const uint64_t t0 = tc::globaltimer_ns();
+    for (uint32_t it = 0;; ++it) {
+        if (ld_acquire(&c->complete) >= target) return true;
+        if (__ldcg(&c->stop) <= target) return false;
+        if ((it & 15u) == 15u) {
+            if (status_now(c) != 0) return false;
+            if (tc::globaltimer_ns() - t0 > kStepperWaitNs) {
+                atomicCAS(&c->status, 0, 4);  // FV_ERR_TIMEOUT
+                return false;
+            }
+            __nanosleep(128);
+        }
+    }
+}
+
+// Warp 0 waits until flag[n] >= target (modulo 2^32) for every dependency n of `tile`.  All 32 lanes
+// call it; the result is the same on every lane.
+__device__ __forceinline__ bool wait_flags(FvCtrl* c, const unsigned* flag, const StepperTiles& st, int tile,
+                                           unsigned target) {
+    const int lane = threadIdx.x & 31;
+    const int b = st.dep_off[tile], e = st.dep_off[tile + 1];
+    const uint64_t t0 = tc::globaltimer_ns();
+    for (uint32_t it = 0;; ++it) {
+        bool mine = true;
+        for (int q = b + lane; q < e; q += 32) mine = mine && int(ld_acquire(flag + st.dep_idx[q]) - target) >= 0;
+        if (__all_sync(0xffffffffu, mine)) return true;
+        if ((it & 15u) == 15u) {
+            const bool stop = status_now(c) != 0 || tc::globaltimer_ns() - t0 > kStepperWaitNs;
+            if (__any_sync(0xffffffffu, stop)) {
+                if (lane == 0 && status_now(c) == 0) atomicCAS(&c->status, 0, 4);
+                return false;
+            }
+            __nanosleep(128);
+        }
+    }
+}
+
+// Publication of a completed step j -- every stage-2 item of step j has finished -- or, at the start
+// of a launch, of j = s0 - 1 for the state the launch starts from.  From the wave speeds and first bad
+// cell of U^{j+1} (reduction slot (j+1) & 1) it decides whether step j+1 runs and with which dt, the
+// loop of main2d.cpp:237-242 (dt = min(compute_dt(U), t_next - t)), records t_{j+2}, clears the slot
+// that step j+1's stage 2 reduces into, counts the step, and releases c->complete = j.  One thread.
+// The decisions are those of stage1_control, so a grid may alternate between the two paths.
+__device__ __forceinline__ void publish_step(FvCtrl* c, const GridDesc& g, long long j) {
+    const int p1 = int((j + 1) & 1);
+    const double t1 = __ldcg(&c->t[p1]);
+    bool run = status_now(c) == 0 && j + 1 < c->s_end;
+    double dt = 0.0;
+    if (run) {
+        if (c->mode == MODE_FIXED) {
+            dt = c->dt_fixed;
+        } else if (!(t1 < c->t_next)) {
+            run = false;
+        } else if (__ldcg(&c->bad[p1]) != INT_MAX) {
+            run = false;
+            c->bad_index = __ldcg(&c->bad[p1]);
+            c->status = 3;  // FV_ERR_NONPHYSICAL
+        } else {
+            const double sx = __longlong_as_double((long long)__ldcg(&c->sxy[p1][0]));
+            const double sy = __longlong_as_double((long long)__ldcg(&c->sxy[p1][1]));
+            dt = smin(g.cfl / (sx / g.dx + sy / g.dy), c->t_next - t1);
+        }
+    }
+    c->srun[p1] = run ? 1 : 0;
+    c->sdt[p1] = dt;
+    if (!run) c->stop = j + 1;  // before the release below: a waiter that sees complete = j sees it
+    if (run) {
+        c->t[p1 ^ 1] = (c->mode == MODE_FIXED) ? t1 : t1 + dt;  // fv_step does not advance the time
+        c->sxy[p1 ^ 1][0] = 0ull;
+        c->sxy[p1 ^ 1][1] = 0ull;
+        c->bad[p1 ^ 1] = INT_MAX;
+    }
+    c->step = j + 1;
+    __threadfence();
+    st_release(&c->complete, j);
+}
+
+// Launch prologue (one small grid before every stepper launch): the queue, the step range, every
+// tile's flags set to "all steps before s0 done", and the publication of step s0 - 1.
+__global__ void stepper_begin_kernel(const GridDesc g, StepperTiles st, long long nsteps) {
+    FvCtrl* c = g.ctrl;
+    const long long s0 = c->step;
+    const int T = st.ntx * st.nty;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        st.flag1[t] = unsigned(s0);
+        st.flag2[t] = unsigned(s0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->queue = 0ull;
+        c->done2 = 0ull;
+        c->s0 = s0;
+        c->s_end = s0 + nsteps;
+        c->stop = LLONG_MAX;
+        publish_step(c, g, s0 - 1);
+    }
+}
+
+template <int FLUX, int LIM, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stepper_kernel(const GridDesc g, const __grid_constant__ TileMaps tm,
+                                                           const StepperTiles st) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destination: 128-byte aligned
+    auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
+    __shared__ double s_dt;
+    __shared__ int s_go, s_tile, s_stage;
+    __shared__ long long s_step;
+    FvCtrl* c = g.ctrl;
+    if (tm.use && threadIdx.x == 0) {
+        tc::mbar_init(&s.bar, 1);
+        tc::fence_mbar_init();
+    }
+    uint32_t phase = 0;
+    for (;;) {
+        // ---- claim the next item and wait for its inputs (warp 0) ----
+        // (launch constants are re-read here rather than kept in registers across the tile body)
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x & 31;
+            const long long T = (long long)st.ntx * st.nty;
+            const long long s0 = c->s0, s_end = c->s_end;  // written by the prologue kernel
+            const bool loop_mode = c->mode == MODE_LOOP;
+            const double t_next = c->t_next;
+            unsigned long long k = 0;
+            if (lane == 0) k = atomicAdd(&c->queue, 1ull);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            const long long step = s0 + (long long)(k / (unsigned long long)(2 * T));
+            const long long r = (long long)(k % (unsigned long long)(2 * T));
+            const int stage = r < T ? 1 : 2;
+            const int tile = int(stage == 1 ? r : r - T);
+            int go = step < s_end;
+            double dt = 0.0;
+            if (go && stage == 1) {
+                if (step > s0) {
+                    // step - 1 must run (else nothing will publish its flags) and, in the loop, step
+                    // must not start at or past t_next; both are known once step - 2 is published
+                    int ok = 1;
+                    if (lane == 0) {
+                        ok = wait_complete(c, step - 2) && __ldcg(&c->srun[(step - 1) & 1]) &&
+                             (!loop_mode || __ldcg(&c->t[step & 1]) < t_next);
+                    }
+                    go = __shfl_sync(0xffffffffu, ok, 0);
+                    if (go) go = wait_flags(c, st.flag2, st, tile, unsigned(step));
+                } else {
+                    go = __ldcg(&c->srun[s0 & 1]);
+                }
+            } else if (go) {
+                int ok = 1;
+                if (lane == 0) {
+                    ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
+                    dt = __ldcg(&c->sdt[step & 1]);
+                }
+                go = __shfl_sync(0xffffffffu, ok, 0);
+                if (go) go = wait_flags(c, st.flag1, st, tile, unsigned(step + 1));
+            }
+            if (lane == 0) {
+                if (go) fence_proxy_async_global();  // before this thread issues the tile's TMA load
+                s_go = go;
+                s_step = step;
+                s_stage = stage;
+                s_tile = tile;
+                s_dt = dt;
+            }
+        }
+        __syncthreads();
+        if (!s_go) return;  // past the launch's last step, the loop has reached t_next, or stopped
+        const int tyi = s_tile / st.ntx, txi = s_tile - tyi * st.ntx;
+        double sx = 0.0, sy = 0.0;
+        int bad = INT_MAX;
+        const int one = 1;
+        auto ctl = []() {};
+        bool done;
+        if (s_stage == 1) {
+            // stage 1 waits for its step's publication only before its update
+            auto pre4 = [&]() -> bool {
+                if (threadIdx.x == 0) {
+                    const long long step = s_step;
+                    const bool ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
+                    s_dt = __ldcg(&c->sdt[step & 1]);
+                    s_go = ok;
+                }
+                __syncthreads();
+                return s_go != 0;
+            };
+            done = tile_body<FLUX, LIM, 1, TX, TY, NT, decltype(ctl), decltype(pre4), true>(
+                g, &tm, phase, txi * TX, tyi * TY, s_dt, one, ctl, s, sx, sy, bad, pre4);
+        } else {
+            done = tile_body<FLUX, LIM, 2, TX, TY, NT, decltype(ctl), NoPre4, true>(g, &tm, phase, txi * TX, tyi * TY,
+                                                                                    s_dt, one, ctl, s, sx, sy, bad);
+        }
+        if (!done) return;  // the step does not run (a bad cell or a timeout stopped the grid)
+        if (s_stage == 2) reduce_wave_speeds<NT>(sx, sy, bad, c, int((s_step + 1) & 1));  // ends with no barrier
+        __syncthreads();  // every store of this item precedes the flag's release
+        if (threadIdx.x == 0) {
+            const long long step = s_step;
+            const int tile = s_tile;
+            fence_proxy_async_global();
+            __threadfence();
+            if (s_stage == 1) {
+                st_release(st.flag1 + tile, unsigned(step + 1));
+            } else {
+                st_release(st.flag2 + tile, unsigned(step + 1));
+                const unsigned long long n = atomicAdd(&c->done2, 1ull) + 1ull;
+                const unsigned long long T = (unsigned long long)st.ntx * st.nty;
+                if (n == (unsigned long long)(step - c->s0 + 1) * T) {
+                    __threadfence();  // every other item's reduction atomics precede their counts
+                    publish_step(c, g, step);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace fv

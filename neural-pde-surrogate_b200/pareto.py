@@ -47,19 +47,21 @@ def truth_frames(items, n, coarse, frames, sizes, log=print):
     ic = importlib.import_module(f"{PKG}.ic")
     s = fv.Solver(fv.make_grid(n, n, 0, 1, 0, 1, "periodic", "periodic"), "hllc", "vanleer", 0.5)
     out, first = [], {m: [] for m in sizes}
+    U = torch.empty((1, n, n, 4), dtype=torch.float64, device="cuda")  # frames stay on the device
     t0 = time.time()
     for fam, idx in items:
         rho, u, v, p, _, params = ic.sample(fam, idx, n)
         t_start = float(params.get("t_start", 0.0))
         s.set_primitive(rho, u, v, p)
         s.advance_to(t_start)
-        U = torch.from_numpy(s.get_state()).cuda()[None]
+        s.get_state(out=U[0])
         for m in sizes:
             first[m].append(block_avg(U, n // m)[0])
         traj = [block_avg(U, n // coarse)[0]]
         for k in range(1, frames + 1):
             s.advance_to(t_start + DT_FRAME * k)
-            traj.append(block_avg(torch.from_numpy(s.get_state()).cuda()[None], n // coarse)[0])
+            s.get_state(out=U[0])
+            traj.append(block_avg(U, n // coarse)[0])
         out.append(torch.stack(traj))
     log(f"truth: {len(items)} trajectories at {n}^2, {frames} frames, {time.time() - t0:.1f} s")
     return torch.stack(out), {m: torch.stack(v).contiguous() for m, v in first.items()}

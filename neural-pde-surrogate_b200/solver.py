@@ -265,10 +265,26 @@ def profile(solver, enable=True):
 
 
 def profile_read(solver):
-    """(mean ms of stage-1 launches, mean ms of stage-2 launches, steps timed) since profile()."""
+    """(mean ms of stage-1 launches, mean ms of stage-2 launches, steps timed) since profile(), for
+    steps taken by the per-stage kernels (fv_step, or fv_advance_to with FV_STEPPER=0)."""
     a, b, n = C.c_double(), C.c_double(), C.c_longlong()
     check(lib().fv_profile_read(solver._h, C.byref(a), C.byref(b), C.byref(n)))
     return a.value, b.value, n.value
+
+
+def profile_steps(solver):
+    """(mean device ms per step, steps timed, stepper launches timed) since profile(), over both
+    kernel paths (fv_profile_steps)."""
+    ms, n, k = C.c_double(), C.c_longlong(), C.c_longlong()
+    check(lib().fv_profile_steps(solver._h, C.byref(ms), C.byref(n), C.byref(k)))
+    return ms.value, n.value, k.value
+
+
+def stepper_tile(solver):
+    """(tile width, height, threads) of the handle's persistent stepper; zeros before its first use."""
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    check(lib().fv_stepper_tile(solver._h, C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value
 
 
 def launch_count(solver):
