@@ -664,6 +664,11 @@ bool valid_common(int flux, int lim, int bc_x, int bc_y) {
 // Lets the library's other translation units report through fv_last_error().
 int fv_internal_set_error(int code, const char* msg) { return set_error(code, "%s", msg ? msg : ""); }
 int fv_internal_encode_maps(const GridDesc& g, int tx, int ty, TileMaps* out) { return encode_maps(g, tx, ty, out); }
+void fv_internal_stepper_deps(int nx, int ny, int bc_x, int bc_y, int tx, int ty, std::vector<int>& off,
+                              std::vector<int>& idx) {
+    build_stepper_deps(nx, ny, bc_x, bc_y, tx, ty, off, idx);
+}
+bool fv_internal_stepper_enabled() { return stepper_enabled(); }
 
 extern "C" {
 

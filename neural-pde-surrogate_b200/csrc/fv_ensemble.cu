@@ -1,11 +1,14 @@
 // Batched ensemble: many independent grids (members) of uneven sizes, each with its own CFL dt, time
 // and step count, advanced together.  The reference runs one process per trajectory (data/generate.py:
-// 60-105, experiments/solver_baseline.py:116-117); here one persistent launch per RK stage covers the
-// tiles of every member still running, and batches of steps are replayed from a captured CUDA graph.
+// 60-105, experiments/solver_baseline.py:116-117); here one persistent cooperative launch (the
+// many-grid stepper of fv_stepper.cuh) advances every member by many steps to its own target time:
+// each member has its own work queue, publication of its dt and tile dependencies, and CTAs move
+// between members as their work runs out.  The launch (prologue + stepper) is captured once in a CUDA
+// graph and replayed per batch.  With FV_STEPPER=0 the members instead advance by one persistent
+// launch per RK stage over the tiles of every running member, replayed in graphs of 16 steps.
 //
-// Each member's arithmetic is the single-grid stage kernel's tile body with that member's own control
-// block (the CTA that handles a member's first tile is its leader), so every member is bit-identical
-// to its own fv_advance_to run.  Members that reached their target time skip their tiles.
+// Each member's arithmetic is the single-grid tile body with that member's own control block, so
+// every member is bit-identical to its own fv_advance_to run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,9 +19,13 @@
 
 #include "../../include/fv.h"
 #include "fv_kernels.cuh"
+#include "fv_stepper.cuh"
 
 int fv_internal_set_error(int code, const char* msg);
 int fv_internal_encode_maps(const fv::GridDesc& g, int tx, int ty, fv::TileMaps* out);
+void fv_internal_stepper_deps(int nx, int ny, int bc_x, int bc_y, int tx, int ty, std::vector<int>& off,
+                              std::vector<int>& idx);
+bool fv_internal_stepper_enabled();
 
 using namespace fv;
 
@@ -89,6 +96,19 @@ __global__ void ensemble_set_kernel(FvCtrl* ctrl, const double* t_next, int coun
 }
 
 using StageFn = void (*)(const GridDesc*, const TileMaps*, const Tile*, int);
+using MultiFn = void (*)(const GridDesc*, const StepperTiles*, const TileMaps*, int, const int*, unsigned*, unsigned*);
+
+template <int F, int L>
+MultiFn multi_of() {
+    return multi_stepper_kernel<F, L, TX, TY, NT, MINB>;
+}
+
+MultiFn multi_kernel(int flux, int lim) {
+    static const MultiFn table[2][4] = {
+        {multi_of<0, 0>(), multi_of<0, 1>(), multi_of<0, 2>(), multi_of<0, 3>()},
+        {multi_of<1, 0>(), multi_of<1, 1>(), multi_of<1, 2>(), multi_of<1, 3>()}};
+    return table[flux][lim];
+}
 
 template <int F, int L>
 void pick(StageFn* s1, StageFn* s2) {
@@ -135,6 +155,19 @@ struct fv_ensemble {
     cudaGraphExec_t graph = nullptr;   // kGraphSteps ensemble steps
     static constexpr int kGraphSteps = 16;
     long long launches = 0;
+    // many-grid stepper: per-member tile tables, all tiles' flags and dependency lists, the first
+    // member of every CTA, members' done marks and the cursor (one device allocation)
+    MultiFn multi = nullptr;
+    void* sbuf = nullptr;
+    StepperTiles* d_stiles = nullptr;
+    int* d_first = nullptr;
+    unsigned* d_done = nullptr;
+    unsigned* d_cursor = nullptr;
+    int sgrid = 0;
+    int total_tiles = 0;
+    cudaGraphExec_t sgraph = nullptr;  // prologue + stepper launch of kStepperSteps steps per member
+    bool stepper_ready = false;
+    static constexpr long long kStepperSteps = 8192;
 };
 
 namespace {
@@ -167,6 +200,103 @@ int build_graph(fv_ensemble* e) {
     cudaGraphDestroy(g);
     if (ce != cudaSuccess) return err(FV_ERR_CUDA, cudaGetErrorString(ce));
     return FV_OK;
+}
+
+cudaError_t enqueue_batch(fv_ensemble* e);
+
+// The many-grid stepper's tables (first use): member m's tiles are entries base_m.. of the flags and
+// dependency lists, and CTA b starts on the member holding tile b * total / grid (largest members get
+// the most CTAs).
+int prepare_stepper(fv_ensemble* e) {
+    e->multi = multi_kernel(e->flux, e->lim);
+    EN_CUDA(cudaFuncSetAttribute((const void*)e->multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
+    int per_sm = 0, dev = 0, sms = 0;
+    EN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, e->multi, NT, sizeof(Smem)));
+    EN_CUDA(cudaGetDevice(&dev));
+    EN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return err(FV_ERR_CUDA, "ensemble stepper cannot be resident");
+    e->sgrid = per_sm * sms;
+    std::vector<StepperTiles> st(e->count);
+    std::vector<int> off(1, 0), idx, base(e->count);
+    for (int m = 0; m < e->count; ++m) {
+        const GridDesc& g = e->h_members[m];
+        std::vector<int> o, ix;
+        fv_internal_stepper_deps(g.nx, g.ny, g.bc_x, g.bc_y, TX, TY, o, ix);
+        base[m] = (int)off.size() - 1;
+        const int i0 = (int)idx.size();
+        for (int v : ix) idx.push_back(v + base[m]);
+        for (size_t t = 1; t < o.size(); ++t) off.push_back(i0 + o[t]);
+        st[m] = StepperTiles{nullptr, nullptr, nullptr, nullptr, (g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, base[m]};
+    }
+    const int T = (int)off.size() - 1;
+    e->total_tiles = T;
+    std::vector<int> first(e->sgrid);
+    for (int b = 0, m = 0; b < e->sgrid; ++b) {
+        const long long tile = (long long)b * T / e->sgrid;
+        while (m + 1 < e->count && base[m + 1] <= tile) ++m;
+        first[b] = m;
+    }
+    const size_t bytes = 2 * size_t(T) * sizeof(unsigned) + (off.size() + idx.size() + first.size()) * sizeof(int) +
+                         e->count * (sizeof(StepperTiles) + sizeof(unsigned)) + 2 * sizeof(unsigned) + 64;
+    EN_CUDA(cudaMalloc(&e->sbuf, bytes));
+    char* p = static_cast<char*>(e->sbuf);
+    e->d_stiles = reinterpret_cast<StepperTiles*>(p);  // first: StepperTiles holds pointers (8-byte alignment)
+    p += e->count * sizeof(StepperTiles);
+    unsigned* flags = reinterpret_cast<unsigned*>(p);
+    p += 2 * size_t(T) * sizeof(unsigned);
+    int* doff = reinterpret_cast<int*>(p);
+    p += off.size() * sizeof(int);
+    int* didx = reinterpret_cast<int*>(p);
+    p += idx.size() * sizeof(int);
+    e->d_first = reinterpret_cast<int*>(p);
+    p += first.size() * sizeof(int);
+    e->d_done = reinterpret_cast<unsigned*>(p);
+    p += e->count * sizeof(unsigned);
+    e->d_cursor = reinterpret_cast<unsigned*>(p);
+    for (auto& x : st) {
+        x.flag1 = flags;
+        x.flag2 = flags + T;
+        x.dep_off = doff;
+        x.dep_idx = didx;
+    }
+    EN_CUDA(cudaMemcpy(e->d_stiles, st.data(), st.size() * sizeof(StepperTiles), cudaMemcpyHostToDevice));
+    EN_CUDA(cudaMemcpy(doff, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+    EN_CUDA(cudaMemcpy(didx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice));
+    EN_CUDA(cudaMemcpy(e->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // the batch launch, captured once: prologue (per-member queues and publications) + stepper; where
+    // the runtime cannot capture a cooperative launch, batches are launched directly
+    cudaGraph_t gr = nullptr;
+    EN_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = enqueue_batch(e);
+    cudaError_t ce2 = cudaStreamEndCapture(e->stream, &gr);
+    if (ce == cudaSuccess && ce2 == cudaSuccess) ce = cudaGraphInstantiate(&e->sgraph, gr, 0);
+    if (gr) cudaGraphDestroy(gr);
+    if (ce != cudaSuccess || ce2 != cudaSuccess) {
+        e->sgraph = nullptr;
+        cudaGetLastError();  // clear the failed capture; the direct launch reports its own errors
+    }
+    e->stepper_ready = true;
+    return FV_OK;
+}
+
+// One batch on the stream: prologue + cooperative many-grid stepper.
+cudaError_t enqueue_batch(fv_ensemble* e) {
+    multi_stepper_begin_kernel<<<std::max(1, std::min((e->count + 127) / 128, 148)), 128, 0, e->stream>>>(
+        e->d_members, e->d_stiles, e->count, e->total_tiles, fv_ensemble::kStepperSteps, e->d_done, e->d_cursor);
+    cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return ce;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: an item's waits always end
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(e->sgrid);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = sizeof(Smem);
+    cfg.stream = e->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, e->multi, (const GridDesc*)e->d_members, (const StepperTiles*)e->d_stiles,
+                              (const TileMaps*)e->d_maps, e->count, (const int*)e->d_first, e->d_done, e->d_cursor);
 }
 
 int read_ctrl(fv_ensemble* e) {
@@ -351,6 +481,8 @@ int fv_ensemble_destroy(fv_ensemble* e) {
     if (!e) return FV_OK;
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->graph) cudaGraphExecDestroy(e->graph);
+    if (e->sgraph) cudaGraphExecDestroy(e->sgraph);
+    cudaFree(e->sbuf);
     cudaFree(e->pool);
     cudaFree(e->ctrl);
     cudaFree(e->d_members);
@@ -406,6 +538,27 @@ int fv_ensemble_state_device(fv_ensemble* e, int m, double** dU) {
     return FV_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// The members' times, step counts and statuses from the control blocks read last.
+int finish_advance(fv_ensemble* e, double* t_out, long long* steps_out, int* status_out) {
+    int worst = FV_OK;
+    for (int m = 0; m < e->count; ++m) {
+        const FvCtrl& c = e->h_ctrl[m];
+        if (t_out) t_out[m] = c.t[c.step & 1];
+        if (steps_out) steps_out[m] = c.step;
+        if (status_out) status_out[m] = c.status;
+        if (c.status) worst = c.status;
+    }
+    if (worst == FV_ERR_TIMEOUT) return err(worst, "fv_ensemble_advance_to: a bounded device wait ran out");
+    if (worst) return err(worst, "fv_ensemble_advance_to: a member reached a non-physical state (see status)");
+    return FV_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int fv_ensemble_advance_to(fv_ensemble* e, const double* t_next, double* t_out, long long* steps_out, int* status_out) {
     if (!e || !t_next) return err(FV_ERR_ARG, "fv_ensemble_advance_to: bad arguments");
     for (int m = 0; m < e->count; ++m)
@@ -415,12 +568,33 @@ int fv_ensemble_advance_to(fv_ensemble* e, const double* t_next, double* t_out, 
     ensemble_set_kernel<<<(e->count + 127) / 128, 128, 0, e->stream>>>(e->ctrl, e->d_tnext, e->count);
     e->launches++;
     EN_CUDA(cudaGetLastError());
-    if (!e->graph) {
-        int rc = build_graph(e);
-        if (rc) return rc;
+    int rc = FV_OK;
+    if (fv_internal_stepper_enabled()) {
+        // one batch (prologue + persistent stepper, a graph replay) advances every member up to
+        // kStepperSteps steps towards its target; a member stops by itself at its t_next or a bad cell
+        if (!e->stepper_ready && (rc = prepare_stepper(e))) return rc;
+        if ((rc = read_ctrl(e))) return rc;
+        for (;;) {
+            bool more = false;
+            for (int m = 0; m < e->count && !more; ++m) {
+                const FvCtrl& c = e->h_ctrl[m];
+                more = !c.status && c.t[c.step & 1] < t_next[m];
+            }
+            if (!more) break;
+            long long before = 0;
+            for (int m = 0; m < e->count; ++m) before += e->h_ctrl[m].step;
+            if (e->sgraph) EN_CUDA(cudaGraphLaunch(e->sgraph, e->stream));
+            else EN_CUDA(enqueue_batch(e));
+            e->launches += 2;
+            if ((rc = read_ctrl(e))) return rc;
+            long long after = 0;
+            for (int m = 0; m < e->count; ++m) after += e->h_ctrl[m].step;
+            if (after == before) break;  // nothing could run (the control blocks stopped every member)
+        }
+        return finish_advance(e, t_out, steps_out, status_out);
     }
-    int rc = read_ctrl(e);
-    if (rc) return rc;
+    if (!e->graph && (rc = build_graph(e))) return rc;
+    if ((rc = read_ctrl(e))) return rc;
     for (;;) {
         // steps still needed by the slowest member, from each member's current CFL dt
         double need = 0.0;
@@ -447,16 +621,7 @@ int fv_ensemble_advance_to(fv_ensemble* e, const double* t_next, double* t_out, 
         }
         if ((rc = read_ctrl(e))) return rc;
     }
-    int worst = FV_OK;
-    for (int m = 0; m < e->count; ++m) {
-        const FvCtrl& c = e->h_ctrl[m];
-        if (t_out) t_out[m] = c.t[c.step & 1];
-        if (steps_out) steps_out[m] = c.step;
-        if (status_out) status_out[m] = c.status;
-        if (c.status) worst = c.status;
-    }
-    if (worst) return err(worst, "fv_ensemble_advance_to: a member reached a non-physical state (see status)");
-    return FV_OK;
+    return finish_advance(e, t_out, steps_out, status_out);
 }
 
 int fv_ensemble_launch_count(fv_ensemble* e, long long* n) {

@@ -50,14 +50,17 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
 // accesses: W and W1 are written by ordinary stores and read by TMA in the same launch.
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
-// Tiles of the stepper's grid and their dependency lists (compressed rows: the dependencies of tile
-// t are dep_idx[dep_off[t] .. dep_off[t+1]), built on the host by build_stepper_deps).
+// Tiles of one grid and their dependency lists.  The arrays may hold the tiles of several grids (an
+// ensemble): a grid's tile t is entry base + t of the flags and of the compressed rows, whose entries
+// dep_idx[dep_off[base + t] .. dep_off[base + t + 1]) are such global tile indices too (built on the
+// host by build_stepper_deps).
 struct StepperTiles {
     unsigned* flag1;       // per tile: number of steps whose stage 1 has finished on it
     unsigned* flag2;       // per tile: number of steps whose stage 2 has finished on it
     const int* dep_off;
     const int* dep_idx;
-    int ntx, nty;
+    int ntx, nty;          // the grid's tiles
+    int base;              // the grid's first tile in the arrays
 };
 
 constexpr unsigned long long kStepperWaitNs = 1000000000ull;  // 1 s: far above any legitimate wait
@@ -89,7 +92,7 @@ __device__ __forceinline__ bool wait_complete(FvCtrl* c, long long target) {
 __device__ __forceinline__ bool wait_flags(FvCtrl* c, const unsigned* flag, const StepperTiles& st, int tile,
                                            unsigned target) {
     const int lane = threadIdx.x & 31;
-    const int b = st.dep_off[tile], e = st.dep_off[tile + 1];
+    const int b = st.dep_off[st.base + tile], e = st.dep_off[st.base + tile + 1];
     const uint64_t t0 = tc::globaltimer_ns();
     for (uint32_t it = 0;; ++it) {
         bool mine = true;
@@ -148,135 +151,221 @@ __device__ __forceinline__ void publish_step(FvCtrl* c, const GridDesc& g, long 
 
 // Launch prologue (one small grid before every stepper launch): the queue, the step range, every
 // tile's flags set to "all steps before s0 done", and the publication of step s0 - 1.
-__global__ void stepper_begin_kernel(const GridDesc g, StepperTiles st, long long nsteps) {
+__device__ __forceinline__ void begin_grid(const GridDesc& g, long long nsteps) {
     FvCtrl* c = g.ctrl;
     const long long s0 = c->step;
+    c->queue = 0ull;
+    c->done2 = 0ull;
+    c->s0 = s0;
+    c->s_end = s0 + nsteps;
+    c->stop = LLONG_MAX;
+    publish_step(c, g, s0 - 1);
+}
+static __global__ void stepper_begin_kernel(const GridDesc g, StepperTiles st, long long nsteps) {
+    const unsigned s0 = unsigned(g.ctrl->step);
     const int T = st.ntx * st.nty;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        st.flag1[t] = unsigned(s0);
-        st.flag2[t] = unsigned(s0);
+        st.flag1[st.base + t] = s0;
+        st.flag2[st.base + t] = s0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        c->queue = 0ull;
-        c->done2 = 0ull;
-        c->s0 = s0;
-        c->s_end = s0 + nsteps;
-        c->stop = LLONG_MAX;
-        publish_step(c, g, s0 - 1);
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) begin_grid(g, nsteps);
 }
 
+// Claims the next item of grid g's queue, waits for its inputs (warp 0), and runs it.  Returns false
+// when the grid has no more items to run in this launch (past its last step, the loop has reached
+// t_next, a bad cell, or a timeout), true after running one.  Called by every thread of the CTA; the
+// mbarrier s.bar (when tm is used) is initialised and `phase` tracks it.
+template <int FLUX, int LIM, int TX, int TY, int NT>
+__device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* tm, const StepperTiles& st,
+                                             TileSmem<TX, TY>& s, uint32_t& phase) {
+    __shared__ double s_dt;
+    __shared__ int s_go, s_tile, s_stage;
+    __shared__ long long s_step;
+    FvCtrl* c = g.ctrl;
+    // ---- claim the next item and wait for its inputs (warp 0) ----
+    // (launch constants are re-read here rather than kept in registers across the tile body)
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x & 31;
+        const long long T = (long long)st.ntx * st.nty;
+        const long long s0 = c->s0, s_end = c->s_end;  // written by the prologue kernel
+        const bool loop_mode = c->mode == MODE_LOOP;
+        const double t_next = c->t_next;
+        unsigned long long k = 0;
+        if (lane == 0) k = atomicAdd(&c->queue, 1ull);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        const long long step = s0 + (long long)(k / (unsigned long long)(2 * T));
+        const long long r = (long long)(k % (unsigned long long)(2 * T));
+        const int stage = r < T ? 1 : 2;
+        const int tile = int(stage == 1 ? r : r - T);
+        int go = step < s_end;
+        double dt = 0.0;
+        if (go && stage == 1) {
+            if (step > s0) {
+                // step - 1 must run (else nothing will publish its flags) and, in the loop, step
+                // must not start at or past t_next; both are known once step - 2 is published
+                int ok = 1;
+                if (lane == 0) {
+                    ok = wait_complete(c, step - 2) && __ldcg(&c->srun[(step - 1) & 1]) &&
+                         (!loop_mode || __ldcg(&c->t[step & 1]) < t_next);
+                }
+                go = __shfl_sync(0xffffffffu, ok, 0);
+                if (go) go = wait_flags(c, st.flag2, st, tile, unsigned(step));
+            } else {
+                go = __ldcg(&c->srun[s0 & 1]);
+            }
+        } else if (go) {
+            int ok = 1;
+            if (lane == 0) {
+                ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
+                dt = __ldcg(&c->sdt[step & 1]);
+            }
+            go = __shfl_sync(0xffffffffu, ok, 0);
+            if (go) go = wait_flags(c, st.flag1, st, tile, unsigned(step + 1));
+        }
+        if (lane == 0) {
+            if (go) fence_proxy_async_global();  // before this thread issues the tile's TMA load
+            s_go = go;
+            s_step = step;
+            s_stage = stage;
+            s_tile = tile;
+            s_dt = dt;
+        }
+    }
+    __syncthreads();
+    if (!s_go) return false;
+    const int tyi = s_tile / st.ntx, txi = s_tile - tyi * st.ntx;
+    double sx = 0.0, sy = 0.0;
+    int bad = INT_MAX;
+    const int one = 1;
+    auto ctl = []() {};
+    bool done;
+    if (s_stage == 1) {
+        // stage 1 waits for its step's publication only before its update
+        auto pre4 = [&]() -> bool {
+            if (threadIdx.x == 0) {
+                const long long step = s_step;
+                const bool ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
+                s_dt = __ldcg(&c->sdt[step & 1]);
+                s_go = ok;
+            }
+            __syncthreads();
+            return s_go != 0;
+        };
+        done = tile_body<FLUX, LIM, 1, TX, TY, NT, decltype(ctl), decltype(pre4), true>(
+            g, tm, phase, txi * TX, tyi * TY, s_dt, one, ctl, s, sx, sy, bad, pre4);
+    } else {
+        done = tile_body<FLUX, LIM, 2, TX, TY, NT, decltype(ctl), NoPre4, true>(g, tm, phase, txi * TX, tyi * TY, s_dt,
+                                                                                one, ctl, s, sx, sy, bad);
+    }
+    if (!done) return false;  // the step does not run (a bad cell or a timeout stopped the grid)
+    if (s_stage == 2) reduce_wave_speeds<NT>(sx, sy, bad, c, int((s_step + 1) & 1));  // ends with no barrier
+    __syncthreads();  // every store of this item precedes the flag's release
+    if (threadIdx.x == 0) {
+        const long long step = s_step;
+        const int tile = st.base + s_tile;
+        fence_proxy_async_global();
+        __threadfence();
+        if (s_stage == 1) {
+            st_release(st.flag1 + tile, unsigned(step + 1));
+        } else {
+            st_release(st.flag2 + tile, unsigned(step + 1));
+            const unsigned long long n = atomicAdd(&c->done2, 1ull) + 1ull;
+            const unsigned long long T = (unsigned long long)st.ntx * st.nty;
+            if (n == (unsigned long long)(step - c->s0 + 1) * T) {
+                __threadfence();  // every other item's reduction atomics precede their counts
+                publish_step(c, g, step);
+            }
+        }
+    }
+    return true;
+}
+
+// One grid: every CTA runs items of the grid's queue until it has none left.
 template <int FLUX, int LIM, int TX, int TY, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stepper_kernel(const GridDesc g, const __grid_constant__ TileMaps tm,
                                                            const StepperTiles st) {
     extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destination: 128-byte aligned
     auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
-    __shared__ double s_dt;
-    __shared__ int s_go, s_tile, s_stage;
-    __shared__ long long s_step;
-    FvCtrl* c = g.ctrl;
     if (tm.use && threadIdx.x == 0) {
         tc::mbar_init(&s.bar, 1);
         tc::fence_mbar_init();
     }
     uint32_t phase = 0;
-    for (;;) {
-        // ---- claim the next item and wait for its inputs (warp 0) ----
-        // (launch constants are re-read here rather than kept in registers across the tile body)
-        if (threadIdx.x < 32) {
-            const int lane = threadIdx.x & 31;
-            const long long T = (long long)st.ntx * st.nty;
-            const long long s0 = c->s0, s_end = c->s_end;  // written by the prologue kernel
-            const bool loop_mode = c->mode == MODE_LOOP;
-            const double t_next = c->t_next;
-            unsigned long long k = 0;
-            if (lane == 0) k = atomicAdd(&c->queue, 1ull);
-            k = __shfl_sync(0xffffffffu, k, 0);
-            const long long step = s0 + (long long)(k / (unsigned long long)(2 * T));
-            const long long r = (long long)(k % (unsigned long long)(2 * T));
-            const int stage = r < T ? 1 : 2;
-            const int tile = int(stage == 1 ? r : r - T);
-            int go = step < s_end;
-            double dt = 0.0;
-            if (go && stage == 1) {
-                if (step > s0) {
-                    // step - 1 must run (else nothing will publish its flags) and, in the loop, step
-                    // must not start at or past t_next; both are known once step - 2 is published
-                    int ok = 1;
-                    if (lane == 0) {
-                        ok = wait_complete(c, step - 2) && __ldcg(&c->srun[(step - 1) & 1]) &&
-                             (!loop_mode || __ldcg(&c->t[step & 1]) < t_next);
-                    }
-                    go = __shfl_sync(0xffffffffu, ok, 0);
-                    if (go) go = wait_flags(c, st.flag2, st, tile, unsigned(step));
-                } else {
-                    go = __ldcg(&c->srun[s0 & 1]);
-                }
-            } else if (go) {
-                int ok = 1;
-                if (lane == 0) {
-                    ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
-                    dt = __ldcg(&c->sdt[step & 1]);
-                }
-                go = __shfl_sync(0xffffffffu, ok, 0);
-                if (go) go = wait_flags(c, st.flag1, st, tile, unsigned(step + 1));
-            }
-            if (lane == 0) {
-                if (go) fence_proxy_async_global();  // before this thread issues the tile's TMA load
-                s_go = go;
-                s_step = step;
-                s_stage = stage;
-                s_tile = tile;
-                s_dt = dt;
-            }
+    while (stepper_item<FLUX, LIM, TX, TY, NT>(g, &tm, st, s, phase)) {
+    }
+}
+
+// Many grids (an ensemble's members), each with its own queue, control block, dt and t_next.  A CTA
+// works on one member until that member has no items left in this launch, then moves to another:
+// first member in proportion to the members' tile counts (first[] on the host), then round-robin
+// from a shared cursor over the members not yet marked done.  An item still waits only on items of
+// its own member claimed before it, each claimed by a resident CTA that finishes it before moving
+// on, so every wait ends.  members, tiles and maps (may be NULL) are per-member arrays.
+template <int FLUX, int LIM, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) multi_stepper_kernel(const GridDesc* __restrict__ members,
+                                                                 const StepperTiles* __restrict__ tiles,
+                                                                 const TileMaps* __restrict__ maps, int count,
+                                                                 const int* __restrict__ first, unsigned* member_done,
+                                                                 unsigned* cursor) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
+    __shared__ int s_member;
+    __shared__ GridDesc s_g;      // the current member's descriptors, read from shared memory as needed
+    __shared__ StepperTiles s_st;
+    if (threadIdx.x == 0) {
+        if (maps) {
+            tc::mbar_init(&s.bar, 1);
+            tc::fence_mbar_init();
         }
-        __syncthreads();
-        if (!s_go) return;  // past the launch's last step, the loop has reached t_next, or stopped
-        const int tyi = s_tile / st.ntx, txi = s_tile - tyi * st.ntx;
-        double sx = 0.0, sy = 0.0;
-        int bad = INT_MAX;
-        const int one = 1;
-        auto ctl = []() {};
-        bool done;
-        if (s_stage == 1) {
-            // stage 1 waits for its step's publication only before its update
-            auto pre4 = [&]() -> bool {
-                if (threadIdx.x == 0) {
-                    const long long step = s_step;
-                    const bool ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
-                    s_dt = __ldcg(&c->sdt[step & 1]);
-                    s_go = ok;
-                }
-                __syncthreads();
-                return s_go != 0;
-            };
-            done = tile_body<FLUX, LIM, 1, TX, TY, NT, decltype(ctl), decltype(pre4), true>(
-                g, &tm, phase, txi * TX, tyi * TY, s_dt, one, ctl, s, sx, sy, bad, pre4);
-        } else {
-            done = tile_body<FLUX, LIM, 2, TX, TY, NT, decltype(ctl), NoPre4, true>(g, &tm, phase, txi * TX, tyi * TY,
-                                                                                    s_dt, one, ctl, s, sx, sy, bad);
-        }
-        if (!done) return;  // the step does not run (a bad cell or a timeout stopped the grid)
-        if (s_stage == 2) reduce_wave_speeds<NT>(sx, sy, bad, c, int((s_step + 1) & 1));  // ends with no barrier
-        __syncthreads();  // every store of this item precedes the flag's release
-        if (threadIdx.x == 0) {
-            const long long step = s_step;
-            const int tile = s_tile;
-            fence_proxy_async_global();
-            __threadfence();
-            if (s_stage == 1) {
-                st_release(st.flag1 + tile, unsigned(step + 1));
-            } else {
-                st_release(st.flag2 + tile, unsigned(step + 1));
-                const unsigned long long n = atomicAdd(&c->done2, 1ull) + 1ull;
-                const unsigned long long T = (unsigned long long)st.ntx * st.nty;
-                if (n == (unsigned long long)(step - c->s0 + 1) * T) {
-                    __threadfence();  // every other item's reduction atomics precede their counts
-                    publish_step(c, g, step);
-                }
-            }
+        s_member = first[blockIdx.x];
+        if (s_member >= 0) {
+            s_g = members[s_member];
+            s_st = tiles[s_member];
         }
     }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        const int m = s_member;
+        if (m < 0) return;
+        if (!stepper_item<FLUX, LIM, TX, TY, NT>(s_g, maps ? maps + m : nullptr, s_st, s, phase)) {
+            if (threadIdx.x == 0) {
+                atomicExch(member_done + m, 1u);
+                const unsigned start = atomicAdd(cursor, 1u);
+                int next = -1;
+                for (int q = 0; q < count && next < 0; ++q) {
+                    const int cand = int((start + unsigned(q)) % unsigned(count));
+                    if (ld_acquire(member_done + cand) == 0u) next = cand;
+                }
+                s_member = next;
+                if (next >= 0) {
+                    s_g = members[next];
+                    s_st = tiles[next];
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Launch prologue of the many-grid stepper: every member's queue, step range and publication, every
+// tile's flags, the members' done marks and the cursor.
+static __global__ void multi_stepper_begin_kernel(const GridDesc* __restrict__ members, const StepperTiles* __restrict__ tiles,
+                                           int count, int total_tiles, long long nsteps, unsigned* member_done,
+                                           unsigned* cursor) {
+    const int stride = gridDim.x * blockDim.x, id = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int m = id; m < count; m += stride) {
+        const StepperTiles& st = tiles[m];
+        const unsigned s0 = unsigned(members[m].ctrl->step);
+        for (int t = 0; t < st.ntx * st.nty; ++t) {
+            st.flag1[st.base + t] = s0;
+            st.flag2[st.base + t] = s0;
+        }
+        member_done[m] = 0u;
+        begin_grid(members[m], nsteps);
+    }
+    if (id == 0) *cursor = 0u;
+    (void)total_tiles;
 }
 
 }  // namespace fv
