@@ -89,6 +89,24 @@ def drift(U, U0):
     return (U.sum(dim=(1, 2)) - U0.sum(dim=(1, 2))) / U0.abs().sum(dim=(1, 2))
 
 
+GAMMA = 1.4
+
+
+def rollout_metrics(pred, true, std):
+    """The reference's rollout metrics (surrogate/rollout.py:54-62) on the GPU, in this build's layout:
+    pred, true (T, n, n, 4) conserved FP64 tensors, std (4,) per-field scales.  Returns
+      rmse       (T, 4)  root mean square error over the grid, divided by std,
+      drift      (T, 4)  total of pred minus the total of true[0], over the total ABSOLUTE amount of
+                         true[0] (the reference's normalisation: net momentum can be ~0),
+      bad_cells  (T,)    cells with rho <= 0 or not p > 0 (a NaN pressure counts as bad)."""
+    rmse = ((pred - true) ** 2).mean(dim=(-3, -2)).sqrt() / std
+    drift = (pred.sum(dim=(-3, -2)) - true[0].sum(dim=(-3, -2))) / true[0].abs().sum(dim=(-3, -2))
+    rho = pred[..., 0]
+    p = (GAMMA - 1) * (pred[..., 3] - 0.5 * (pred[..., 1] ** 2 + pred[..., 2] ** 2) / rho)
+    bad = ((rho <= 0) | ~(p > 0)).sum(dim=(-2, -1))
+    return {"rmse": rmse, "drift": drift, "bad_cells": bad}
+
+
 def run_plain(first, n, coarse, frames, truth, families=None):
     """All test trajectories at n^2 in one fv_ensemble; errors on the coarse grid."""
     import torch

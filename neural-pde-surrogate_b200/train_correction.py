@@ -221,8 +221,9 @@ def train(cfg, log=print):
         log(f"dataset: packed {cfg['packed']}: train {tuple(train_U.shape[:2])}, val {tuple(val_U.shape[:2])} "
             f"(trajectories, frames) at {cfg['coarse']}^2")
     else:
-        train_U = build_dataset(cfg["n_traj"], cfg["fine"], cfg["coarse"], index0=0, log=log)
-        val_U = build_dataset(cfg["n_val"], cfg["fine"], cfg["coarse"], index0=100000, log=log)
+        fams = tuple(cfg.get("families") or ("riemann", "blast"))
+        train_U = build_dataset(cfg["n_traj"], cfg["fine"], cfg["coarse"], index0=0, families=fams, log=log)
+        val_U = build_dataset(cfg["n_val"], cfg["fine"], cfg["coarse"], index0=100000, families=fams, log=log)
     tr = Trainer(train_U, val_U, cfg["batch"], cfg["unroll"], seed=cfg["seed"], log=log, init=cfg.get("init"))
     tr.noise = float(cfg.get("noise", 0.0))
     corr = tr.corr
