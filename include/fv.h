@@ -179,6 +179,15 @@ int fv_division_sweep(int kind, long long n, unsigned long long seed, long long*
  * stored by the solver itself).  Ug: host array of (ny+4)*(nx+4)*4 doubles. */
 int fv_fill_ghosts(int nx, int ny, int bc_x, int bc_y, const double* U, double* Ug);
 
+/* The persistent stepper's dependency lists for an nx x ny grid of tx x ty tiles (host code, no GPU
+ * needed): for tile t (row-major over tiles), idx[off[t] .. off[t+1]) are the tiles holding a cell of
+ * its halo box [i0-2, i0+tx+1] x [j0-2, j0+ty+1] once mapped through the boundary conditions
+ * (grid2d.hpp:43-66), and the tiles whose halo box holds one of its cells, itself included, sorted.
+ * *nnz receives the number of entries; off (ntiles + 1 entries) and idx are filled when their
+ * capacities suffice.  Inspection hook; no reference counterpart. */
+int fv_stepper_dependencies(int nx, int ny, int bc_x, int bc_y, int tx, int ty, int* off, int off_cap, int* idx,
+                            int idx_cap, int* nnz);
+
 /* Tile shapes.  The stage kernels exist for several CTA tile shapes (fv_tile_variant enumerates
  * them: tile width, height, threads); all give bit-identical results.  A handle picks the fastest
  * for its grid by timing each on a copy of its state the first time it steps (the autotuner; the

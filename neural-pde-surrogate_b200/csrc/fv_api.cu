@@ -1042,6 +1042,18 @@ int fv_fill_ghosts(int nx, int ny, int bc_x, int bc_y, const double* U, double* 
     return FV_OK;
 }
 
+int fv_stepper_dependencies(int nx, int ny, int bc_x, int bc_y, int tx, int ty, int* off, int off_cap, int* idx,
+                            int idx_cap, int* nnz) {
+    if (nx <= 0 || ny <= 0 || tx <= 0 || ty <= 0 || !nnz) return set_error(FV_ERR_ARG, "fv_stepper_dependencies: bad arguments");
+    if (!valid_common(FLUX_HLLC, LIM_NONE, bc_x, bc_y)) return set_error(FV_ERR_ARG, "fv_stepper_dependencies: unknown bc");
+    std::vector<int> o, ix;
+    build_stepper_deps(nx, ny, bc_x, bc_y, tx, ty, o, ix);
+    *nnz = (int)ix.size();
+    if (off && off_cap >= (int)o.size()) std::memcpy(off, o.data(), o.size() * sizeof(int));
+    if (idx && idx_cap >= (int)ix.size()) std::memcpy(idx, ix.data(), ix.size() * sizeof(int));
+    return FV_OK;
+}
+
 int fv_autotune(fv_solver* s, int steps, int* variant) {
     if (!s) return set_error(FV_ERR_ARG, "fv_autotune: NULL handle");
     if (!s->has_state) return set_error(FV_ERR_STATE, "fv_autotune: no state set");
