@@ -118,6 +118,7 @@ const std::vector<StepperVariant>& stepper_variants() {
         StepperMaker<32, 8, 256, 4>::make(0),   // 2
         StepperMaker<16, 7, 128, 8>::make(8),   // 3
         StepperMaker<32, 16, 512, 2>::make(1),  // 4
+        StepperMaker<16, 7, 128, 9>::make(10),  // 5: 36 warps per SM at <= 56 registers
     };
     return v;
 }

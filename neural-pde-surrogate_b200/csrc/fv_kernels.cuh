@@ -291,45 +291,51 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
     if (!go) return false;
     FV_PHASE_MARK(1);
 
-    // P2: limited slopes
-    for (int e = threadIdx.x; e < NSX + NSY; e += NT) {
-        if (e < NSX) {
-            const int r = e / (TX + 2), k = e - r * (TX + 2);  // cell (k-1, r) = W[r+2][k+1]
-            sts(s.dX, r, k, limited_slope<LIM>(lds(s.W, r + 2, k), lds(s.W, r + 2, k + 1), lds(s.W, r + 2, k + 2)));
-        } else {
-            const int e2 = e - NSX;
-            const int r = e2 / TX, k = e2 - r * TX;  // cell (k, r-1) = W[r+1][k+2]
-            sts(s.dY, r, k, limited_slope<LIM>(lds(s.W, r, k + 2), lds(s.W, r + 1, k + 2), lds(s.W, r + 2, k + 2)));
+    // P2: limited slopes.  x-slopes of cells -1..TX per row, y-slopes of rows -1..TY per column.
+    auto slope_x = [&](int e) {
+        const int r = e / (TX + 2), k = e - r * (TX + 2);  // cell (k-1, r) = W[r+2][k+1]
+        sts(s.dX, r, k, limited_slope<LIM>(lds(s.W, r + 2, k), lds(s.W, r + 2, k + 1), lds(s.W, r + 2, k + 2)));
+    };
+    auto slope_y = [&](int e) {
+        const int r = e / TX, k = e - r * TX;  // cell (k, r-1) = W[r+1][k+2]
+        sts(s.dY, r, k, limited_slope<LIM>(lds(s.W, r, k + 2), lds(s.W, r + 1, k + 2), lds(s.W, r + 2, k + 2)));
+    };
+    // Where each direction fits in as many rounds of the CTA's threads as both together, the two
+    // directions run as separate loops (uniform code per loop); otherwise as one loop over both.
+    if constexpr ((NSX + NT - 1) / NT + (NSY + NT - 1) / NT == (NSX + NSY + NT - 1) / NT) {
+        for (int e = threadIdx.x; e < NSX; e += NT) slope_x(e);
+        for (int e = threadIdx.x; e < NSY; e += NT) slope_y(e);
+    } else {
+        for (int e = threadIdx.x; e < NSX + NSY; e += NT) {
+            if (e < NSX) slope_x(e);
+            else slope_y(e - NSX);
         }
     }
     __syncthreads();
     FV_PHASE_MARK(2);
 
     // P3: face fluxes, flux(to_conserved(edge(W_L, dW_L, +1)), to_conserved(edge(W_R, dW_R, -1))),
-    // with each side's to_primitive by face_side
-    for (int e = threadIdx.x; e < NFX + NFY; e += NT) {
-        Q4 wl, dl, wr, dr;
-        const bool ydir = e >= NFX;
-        int r, k;
-        if (!ydir) {  // x-face k of row r, between cells k-1 and k (solver2d.hpp:145-148)
-            r = e / (TX + 1); k = e - r * (TX + 1);
-            wl = lds(s.W, r + 2, k + 1); dl = lds(s.dX, r, k);
-            wr = lds(s.W, r + 2, k + 2); dr = lds(s.dX, r, k + 1);
-        } else {      // y-face r of column k, between rows r-1 and r (solver2d.hpp:165-169)
-            const int e2 = e - NFX;
-            r = e2 / TX; k = e2 - r * TX;
-            wl = lds(s.W, r + 1, k + 2); dl = lds(s.dY, r, k);
-            wr = lds(s.W, r + 2, k + 2); dr = lds(s.dY, r + 1, k);
+    // with each side's to_primitive by face_side; the y-faces through the momentum swap
+    auto face_x = [&](int e) {  // x-face k of row r, between cells k-1 and k (solver2d.hpp:145-148)
+        const int r = e / (TX + 1), k = e - r * (TX + 1);
+        const FaceSide L = face_side(edge(lds(s.W, r + 2, k + 1), lds(s.dX, r, k), +1.0));
+        const FaceSide R = face_side(edge(lds(s.W, r + 2, k + 2), lds(s.dX, r, k + 1), -1.0));
+        sts(s.F, r, k, face_flux<FLUX>(L.U, L.W, R.U, R.W));
+    };
+    auto face_y = [&](int e) {  // y-face r of column k, between rows r-1 and r (solver2d.hpp:165-169)
+        const int r = e / TX, k = e - r * TX;
+        const FaceSide L = face_side(edge(lds(s.W, r + 1, k + 2), lds(s.dY, r, k), +1.0));
+        const FaceSide R = face_side(edge(lds(s.W, r + 2, k + 2), lds(s.dY, r + 1, k), -1.0));
+        sts(s.G, r, k, swap_xy(face_flux<FLUX>(swap_xy(L.U), swap_xy(L.W), swap_xy(R.U), swap_xy(R.W))));
+    };
+    if constexpr ((NFX + NT - 1) / NT + (NFY + NT - 1) / NT == (NFX + NFY + NT - 1) / NT) {
+        for (int e = threadIdx.x; e < NFX; e += NT) face_x(e);
+        for (int e = threadIdx.x; e < NFY; e += NT) face_y(e);
+    } else {
+        for (int e = threadIdx.x; e < NFX + NFY; e += NT) {
+            if (e < NFX) face_x(e);
+            else face_y(e - NFX);
         }
-        FaceSide L = face_side(edge(wl, dl, +1.0));
-        FaceSide R = face_side(edge(wr, dr, -1.0));
-        if (ydir) {
-            L.U = swap_xy(L.U); L.W = swap_xy(L.W);
-            R.U = swap_xy(R.U); R.W = swap_xy(R.W);
-        }
-        Q4 F = face_flux<FLUX>(L.U, L.W, R.U, R.W);
-        if (ydir) sts(s.G, r, k, swap_xy(F));
-        else sts(s.F, r, k, F);
     }
     __syncthreads();
     FV_PHASE_MARK(3);
