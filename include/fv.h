@@ -221,6 +221,14 @@ int fv_stepper_tile(fv_solver* s, int* tx, int* ty, int* threads);
  * did not, FV_ERR_CUDA on a CUDA error.  No reference counterpart (the reference has no GPU code). */
 int fv_wait_selftest(void);
 
+/* Self-test of the persistent stepper's bounded waits: its wait for a step's publication and its
+ * wait for neighbour tiles' flags, each run against a control block and a flag that nothing ever
+ * publishes, with a 10 ms limit, plus a second CTA waiting with the default limit that must leave as
+ * soon as the first has recorded the timeout.  Returns FV_ERR_TIMEOUT when every wait gave up and
+ * reported it (the expected outcome; the context stays usable), FV_ERR_STATE if not, FV_ERR_CUDA on
+ * a CUDA error.  No reference counterpart. */
+int fv_stepper_wait_selftest(void);
+
 /* Measured FP64 FMA throughput of the current device (DFMA per second, one FMA = 2 flops): the
  * denominator of the FP64-pipe roofline the stage kernels are reported against.  No reference
  * counterpart (the reference has no GPU code). */

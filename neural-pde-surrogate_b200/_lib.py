@@ -66,6 +66,7 @@ _PROTOS = {
     "fv_launch_count": [_P, _LLP],
     "fv_fp64_peak": [_DP],
     "fv_wait_selftest": [],
+    "fv_stepper_wait_selftest": [],
     "fv_ensemble_create": [_I, _P, _P, _P, _P, _P, _I, _I, _D, _P, C.POINTER(_P)],
     "fv_ensemble_destroy": [_P],
     "fv_ensemble_set_state": [_P, _I, _P],

@@ -45,6 +45,62 @@ extern "C" int fv_wait_selftest(void) {
     return (h[0] == 1 && h[1] == 2) ? FV_ERR_TIMEOUT : FV_ERR_STATE;
 }
 
+// ---- the persistent stepper's waits ---------------------------------------------------------------
+// The stepper's two waits -- for a step's publication and for the neighbour tiles' flags -- run here
+// against control blocks and a flag that nothing will ever publish, each with a 10 ms limit: each
+// must give up and record FV_ERR_TIMEOUT in its control block.  A second CTA waits on the flags'
+// control block with the default 1 s limit and must leave as soon as it sees that status.
+#include "fv_stepper.cuh"
+
+namespace {
+
+// Device memory of the test: two control blocks, then one flag (never set), the dependency list of
+// a single tile on itself (offsets {0, 1}, index {0}) and three outcomes.
+struct WaitTest {
+    fv::FvCtrl c[2];
+    unsigned flag;
+    int dep[3];
+    int outcome[3];
+};
+
+__global__ void stepper_wait_selftest_kernel(WaitTest* w) {
+    const fv::StepperTiles st{&w->flag, &w->flag, w->dep, w->dep + 2, 1, 1, 0};
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) w->outcome[0] = fv::wait_complete(&w->c[0], 5, 10000000ull) ? 1 : 2;
+        __syncwarp();
+        const bool ok = fv::wait_flags(&w->c[1], &w->flag, st, 0, 7u, 10000000ull);
+        if (threadIdx.x == 0) w->outcome[1] = ok ? 1 : 2;
+    } else {
+        const uint64_t t0 = tc::globaltimer_ns();
+        const bool ok = fv::wait_flags(&w->c[1], &w->flag, st, 0, 7u);
+        if (threadIdx.x == 0) w->outcome[2] = ok ? 1 : (tc::globaltimer_ns() - t0 < 500000000ull ? 2 : 3);
+    }
+}
+
+}  // namespace
+
+extern "C" int fv_stepper_wait_selftest(void) {
+    WaitTest h{};
+    for (auto& c : h.c) {
+        c.complete = -1;       // no step published
+        c.stop = LLONG_MAX;    // and none known not to run
+    }
+    h.dep[1] = 1;              // offsets {0, 1}, index {0}
+    WaitTest* d = nullptr;
+    if (cudaMalloc(&d, sizeof(WaitTest)) != cudaSuccess) return FV_ERR_CUDA;
+    cudaError_t e = cudaMemcpy(d, &h, sizeof h, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        stepper_wait_selftest_kernel<<<2, 32>>>(d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return FV_ERR_CUDA;
+    const bool gave_up = h.outcome[0] == 2 && h.outcome[1] == 2 && h.outcome[2] == 2;
+    return (gave_up && h.c[0].status == FV_ERR_TIMEOUT && h.c[1].status == FV_ERR_TIMEOUT) ? FV_ERR_TIMEOUT
+                                                                                           : FV_ERR_STATE;
+}
+
 // ---- the divisions of the stage kernels against IEEE division -------------------------------------
 // The stage kernels replace IEEE a / b by cheaper sequences where those give the same quotient:
 // div_gm1 (p / (GAMMA - 1)), div_z (zero numerators), div_back (a face state's velocity after the

@@ -71,14 +71,14 @@ __device__ __forceinline__ int status_now(const FvCtrl* c) { return __ldcg(&c->s
 // it never will be -- an earlier step does not run (c->stop <= target: t_next reached, a bad cell, or
 // the launch's last step) -- on a timeout (recorded as FV_ERR_TIMEOUT), or when another CTA has
 // stopped the grid.
-__device__ __forceinline__ bool wait_complete(FvCtrl* c, long long target) {
+__device__ __forceinline__ bool wait_complete(FvCtrl* c, long long target, uint64_t limit_ns = kStepperWaitNs) {
     const uint64_t t0 = tc::globaltimer_ns();
     for (uint32_t it = 0;; ++it) {
         if (ld_acquire(&c->complete) >= target) return true;
         if (__ldcg(&c->stop) <= target) return false;
         if ((it & 15u) == 15u) {
             if (status_now(c) != 0) return false;
-            if (tc::globaltimer_ns() - t0 > kStepperWaitNs) {
+            if (tc::globaltimer_ns() - t0 > limit_ns) {
                 atomicCAS(&c->status, 0, 4);  // FV_ERR_TIMEOUT
                 return false;
             }
@@ -90,7 +90,7 @@ __device__ __forceinline__ bool wait_complete(FvCtrl* c, long long target) {
 // Warp 0 waits until flag[n] >= target (modulo 2^32) for every dependency n of `tile`.  All 32 lanes
 // call it; the result is the same on every lane.
 __device__ __forceinline__ bool wait_flags(FvCtrl* c, const unsigned* flag, const StepperTiles& st, int tile,
-                                           unsigned target) {
+                                           unsigned target, uint64_t limit_ns = kStepperWaitNs) {
     const int lane = threadIdx.x & 31;
     const int b = st.dep_off[st.base + tile], e = st.dep_off[st.base + tile + 1];
     const uint64_t t0 = tc::globaltimer_ns();
@@ -99,7 +99,7 @@ __device__ __forceinline__ bool wait_flags(FvCtrl* c, const unsigned* flag, cons
         for (int q = b + lane; q < e; q += 32) mine = mine && int(ld_acquire(flag + st.dep_idx[q]) - target) >= 0;
         if (__all_sync(0xffffffffu, mine)) return true;
         if ((it & 15u) == 15u) {
-            const bool stop = status_now(c) != 0 || tc::globaltimer_ns() - t0 > kStepperWaitNs;
+            const bool stop = status_now(c) != 0 || tc::globaltimer_ns() - t0 > limit_ns;
             if (__any_sync(0xffffffffu, stop)) {
                 if (lane == 0 && status_now(c) == 0) atomicCAS(&c->status, 0, 4);
                 return false;
