@@ -320,13 +320,13 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
         const int r = e / (TX + 1), k = e - r * (TX + 1);
         const FaceSide L = face_side(edge(lds(s.W, r + 2, k + 1), lds(s.dX, r, k), +1.0));
         const FaceSide R = face_side(edge(lds(s.W, r + 2, k + 2), lds(s.dX, r, k + 1), -1.0));
-        sts(s.F, r, k, face_flux<FLUX>(L.U, L.W, R.U, R.W));
+        sts(s.F, r, k, face_flux<FLUX>(L, R));
     };
     auto face_y = [&](int e) {  // y-face r of column k, between rows r-1 and r (solver2d.hpp:165-169)
         const int r = e / TX, k = e - r * TX;
         const FaceSide L = face_side(edge(lds(s.W, r + 1, k + 2), lds(s.dY, r, k), +1.0));
         const FaceSide R = face_side(edge(lds(s.W, r + 2, k + 2), lds(s.dY, r + 1, k), -1.0));
-        sts(s.G, r, k, swap_xy(face_flux<FLUX>(swap_xy(L.U), swap_xy(L.W), swap_xy(R.U), swap_xy(R.W))));
+        sts(s.G, r, k, swap_xy(face_flux<FLUX>(swapped(L), swapped(R))));
     };
     if constexpr ((NFX + NT - 1) / NT + (NFY + NT - 1) / NT == (NFX + NFY + NT - 1) / NT) {
         for (int e = threadIdx.x; e < NFX; e += NT) face_x(e);

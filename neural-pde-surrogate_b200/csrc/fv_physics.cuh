@@ -82,6 +82,15 @@ __device__ __forceinline__ double fdiv(double a, double b) {
     const double q = a * y;
     return fma(fma(-q, b, a), y, q);
 }
+// 1/b for divisions that share a denominator: the same seed and two Newton-Raphson steps (a quotient
+// a * recip(b) is then within about 1.5 ulp); operands outside 2^-500 < |b| < 2^500 take `/`.
+__device__ __forceinline__ double recip(double b) {
+    if (!(fabs(b) > 0x1p-500 && fabs(b) < 0x1p+500)) return 1.0 / b;
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    y = fma(y, fma(-b, y, 1.0), y);
+    return fma(y, fma(-b, y, 1.0), y);
+}
 #endif
 
 // a / b with a fast path for a zero numerator (zero velocities in a fluid at rest, equal left and
@@ -121,31 +130,41 @@ __device__ __forceinline__ Q4 to_conserved(const Q4& W) {
 
 // state2d.hpp:21-25
 __device__ __forceinline__ Q4 to_primitive(const Q4& U) {
+#ifndef FV_TOLERANCE_BUILD
     double u = div_z(U.b, U.a), v = div_z(U.c, U.a);
+#else
+    const double r = recip(U.a);  // one reciprocal for both velocities
+    double u = U.b * r, v = U.c * r;
+#endif
     double p = GM1 * (U.d - 0.5 * U.a * (u * u + v * v));
     return Q4{U.a, u, v, p};
 }
 
-// One side of a face: U = to_conserved(We) of the MUSCL edge state We, and W = to_primitive(U), the
-// primitive state the reference's flux function recomputes from U (riemann2d.hpp:12,28).  The
-// velocities come from div_back (same bits as the divisions of to_primitive); the pressure is
-// to_primitive's expression on them.  The tolerance build keeps the edge state itself as W (within
-// an ulp per component of the round trip) and skips the recomputation.
+// state2d.hpp:27
+__device__ __forceinline__ double sound_speed(const Q4& W) { return sqrt(fdiv(GAMMA * W.d, W.a)); }
+
+// One side of a face: U = to_conserved(We) of the MUSCL edge state We, W = to_primitive(U), the
+// primitive state the reference's flux function recomputes from U (riemann2d.hpp:12,28), and its
+// sound speed a = sound_speed(W), which both flux functions evaluate once per side (riemann2d.hpp:13,
+// 29).  The velocities come from div_back (same bits as the divisions of to_primitive); the pressure
+// and the sound speed are the reference's expressions on them.  The tolerance build keeps the edge
+// state itself as W (within an ulp per component of the round trip), and r = 1/rho is shared by
+// the side's divisions by rho.
 struct FaceSide {
     Q4 U, W;
+    double a, r;  // r: tolerance build only
 };
 __device__ __forceinline__ FaceSide face_side(const Q4& We) {
     const Q4 U = to_conserved(We);
 #ifndef FV_TOLERANCE_BUILD
     const double u = div_back(U.b, We.a, We.b), v = div_back(U.c, We.a, We.c);
-    return FaceSide{U, Q4{U.a, u, v, GM1 * (U.d - 0.5 * U.a * (u * u + v * v))}};
+    const Q4 W{U.a, u, v, GM1 * (U.d - 0.5 * U.a * (u * u + v * v))};
+    return FaceSide{U, W, sound_speed(W), 0.0};
 #else
-    return FaceSide{U, We};
+    const double r = recip(We.a);
+    return FaceSide{U, We, sqrt(GAMMA * We.d * r), r};
 #endif
 }
-
-// state2d.hpp:27
-__device__ __forceinline__ double sound_speed(const Q4& W) { return sqrt(fdiv(GAMMA * W.d, W.a)); }
 
 // state2d.hpp:30-36, with the primitive state of U supplied by the caller (it is the same
 // to_primitive(U) the reference recomputes, so reusing it is bit-identical).
@@ -182,9 +201,10 @@ __device__ __forceinline__ Q4 edge(const Q4& W, const Q4& dW, double s) {
     return Q4{W.a + h * dW.a, W.b + h * dW.b, W.c + h * dW.c, W.d + h * dW.d};
 }
 
-// riemann2d.hpp:11-15, given WL = to_primitive(UL) and WR = to_primitive(UR)
-__device__ __forceinline__ Q4 rusanov_flux(const Q4& UL, const Q4& WL, const Q4& UR, const Q4& WR) {
-    double s_max = smax(fabs(WL.b) + sound_speed(WL), fabs(WR.b) + sound_speed(WR));
+// riemann2d.hpp:11-15, on two face sides (conserved state, its primitive state and sound speed)
+__device__ __forceinline__ Q4 rusanov_flux(const FaceSide& L, const FaceSide& R) {
+    const Q4 &UL = L.U, &WL = L.W, &UR = R.U, &WR = R.W;
+    double s_max = smax(fabs(WL.b) + L.a, fabs(WR.b) + R.a);
     Q4 FL = flux_x(UL, WL), FR = flux_x(UR, WR);
     double h = 0.5 * s_max;
     return Q4{0.5 * (FL.a + FR.a) - h * (UR.a - UL.a), 0.5 * (FL.b + FR.b) - h * (UR.b - UL.b),
@@ -196,8 +216,9 @@ __device__ __forceinline__ Q4 rusanov_flux(const Q4& UL, const Q4& WL, const Q4&
 // (left when 0 <= SL or 0 <= S_star, as its first two branches are) and the star state is evaluated
 // once for that side, so that all lanes of a warp run one code path.  Every branch returns the same
 // expression on the same inputs as the reference, hence bit-identical results.
-__device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& WL, const Q4& UR, const Q4& WR) {
-    double aL = sound_speed(WL), aR = sound_speed(WR);
+__device__ __forceinline__ Q4 hllc_flux(const FaceSide& L, const FaceSide& R) {
+    const Q4 &UL = L.U, &WL = L.W, &UR = R.U, &WR = R.W;
+    const double aL = L.a, aR = R.a;
     double SL = smin(WL.b - aL, WR.b - aR);
     double SR = smax(WL.b + aL, WR.b + aR);
     double S_star = div_z(WR.d - WL.d + WL.a * WL.b * (SL - WL.b) - WR.a * WR.b * (SR - WR.b),
@@ -209,22 +230,42 @@ __device__ __forceinline__ Q4 hllc_flux(const Q4& UL, const Q4& WL, const Q4& UR
     Q4 F = flux_x(U, W);
     if (0.0 <= SL || !(left || 0.0 <= SR)) return F;   // pure upwind: F(UL) if 0<=SL, F(UR) if SR<0
     double factor = div_z(W.a * (S - W.b), S - S_star);
+#ifndef FV_TOLERANCE_BUILD
+    const double e_rho = fdiv(U.d, W.a);
+#else
+    const double e_rho = U.d * (left ? L.r : R.r);  // E / rho with the side's reciprocal
+#endif
     Q4 st{factor, factor * S_star, factor * W.c,
-          factor * (fdiv(U.d, W.a) + (S_star - W.b) * (S_star + fdiv(W.d, W.a * (S - W.b))))};
+          factor * (e_rho + (S_star - W.b) * (S_star + fdiv(W.d, W.a * (S - W.b))))};
     return Q4{F.a + S * (st.a - U.a), F.b + S * (st.b - U.b), F.c + S * (st.c - U.c), F.d + S * (st.d - U.d)};
 }
 
 // Flux scheme chosen at compile time (one kernel instance per scheme), on two face sides.
 template <int FLUX>
-__device__ __forceinline__ Q4 face_flux(const Q4& UL, const Q4& WL, const Q4& UR, const Q4& WR) {
-    if constexpr (FLUX == FLUX_HLLC) return hllc_flux(UL, WL, UR, WR);
-    else return rusanov_flux(UL, WL, UR, WR);
+__device__ __forceinline__ Q4 face_flux(const FaceSide& L, const FaceSide& R) {
+    if constexpr (FLUX == FLUX_HLLC) return hllc_flux(L, R);
+    else return rusanov_flux(L, R);
 }
 
-// The FluxFn interface itself (riemann2d.hpp:8): conserved states in, primitives recomputed.
+// A face side from a conserved state alone: the FluxFn interface (riemann2d.hpp:8), which
+// recomputes the primitive state and sound speed from U.
+__device__ __forceinline__ FaceSide side_of(const Q4& U) {
+    const Q4 W = to_primitive(U);
+#ifndef FV_TOLERANCE_BUILD
+    return FaceSide{U, W, sound_speed(W), 0.0};
+#else
+    const double r = recip(U.a);
+    return FaceSide{U, W, sqrt(GAMMA * W.d * r), r};
+#endif
+}
 template <int FLUX>
 __device__ __forceinline__ Q4 face_flux(const Q4& UL, const Q4& UR) {
-    return face_flux<FLUX>(UL, to_primitive(UL), UR, to_primitive(UR));
+    return face_flux<FLUX>(side_of(UL), side_of(UR));
+}
+
+// The same face seen by a y-face: the momentum components swapped (flux_y_face, riemann2d.hpp:42-44).
+__device__ __forceinline__ FaceSide swapped(const FaceSide& f) {
+    return FaceSide{Q4{f.U.a, f.U.c, f.U.b, f.U.d}, Q4{f.W.a, f.W.c, f.W.b, f.W.d}, f.a, f.r};
 }
 
 // state2d.hpp:39
