@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "../../include/fvnet.h"
 #include "tc_sm100.cuh"
@@ -169,6 +170,132 @@ __global__ void __launch_bounds__(NT) conv3x3_kernel(ConvArgs a) {
                     for (int j = 0; j < 8; ++j) {
                         const float gz = (MODE == FVNET_CONV_BWD_GELU) ? gelu_tanh_grad(__bfloat162float(zb[j])) : 1.0f;
                         d[8 * q + j] = acc[8 * q + j] * gz;
+                    }
+                }
+                uint4* Ao = reinterpret_cast<uint4*>(a.A + gp * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) Ao[q] = pack8(d + 8 * q);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+}
+
+// ---- forward / backward data, one staged copy (image widths >= 64) -------------------------------
+// The same implicit GEMM with a quarter of the shared memory, so that more CTAs (warps) fit per SM:
+// the rows y0-1 .. y0+TR are staged once, each row padded with its periodic neighbours
+// ([cc][row][x = -1, 0, .., W-1, W][8]), and the x-shift kx - 1 of a 64-pixel M-tile is a start
+// offset of kx pixels (16 bytes each) in the MMA descriptor.  An M-tile is 64 output pixels of one
+// row (W >= 64), so the MMAs are M = 64: the 1-CTA M = 64 accumulator puts its rows 16q .. 16q+15 in
+// TMEM lanes 32q .. 32q+15, and a second tile whose address starts at lane 16 takes lanes
+// 32q+16 .. 32q+31 (the interleaved layout), so two tiles share one set of COUT columns and a
+// 32-lane tcgen05.ld gives each warp 16 pixels of each.  The CTA's 256 pixels are 4 tiles in 2
+// column sets.
+__host__ __device__ constexpr int rows_plane(int W) {  // padded pixels per channel chunk, = 1 (mod 8)
+    return (((256 / W + 2) * (W + 2) + 7) / 8) * 8 + 1;
+}
+__host__ __device__ constexpr size_t rows_smem_bytes(int cin, int cout, int W) {
+    // at least 29 KB: at most 7 CTAs per SM, so that their TMEM (64 columns each) always fits
+    const size_t b = size_t(cin / 8) * rows_plane(W) * 16 + size_t(9) * (cin / 8) * cout * 16 + 64;
+    return b < 29 * 1024 ? 29 * 1024 : b;
+}
+
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(NT) conv3x3_rows_kernel(ConvArgs a) {
+    constexpr int CC = CIN / 8;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int W = a.W, H = a.H;
+    const int TR = 256 / W, W2 = W + 2, PS = rows_plane(W), TPR = W / 64;
+    uint4* Xs = reinterpret_cast<uint4*>(smem);   // [CC][PS]: rows of W + 2 padded pixels
+    uint4* Wt = Xs + size_t(CC) * PS;              // [9][CC][COUT]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Wt + 9 * CC * COUT);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n = blockIdx.y, y0 = blockIdx.x * TR;
+    constexpr uint32_t kCols = (2 * COUT) < 32 ? 32 : 2 * COUT;
+
+    if (warp == 0) tc::tmem_alloc(tslot, kCols);
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    // stage rows y0-1 .. y0+TR (periodic in y) once, with the periodic x-neighbours at both ends
+#pragma unroll 4
+    for (int e = tid; e < (TR + 2) * W * CC; e += NT) {
+        const int cc = e % CC, t = e / CC, x = t % W, r = t / W;
+        const int y = (y0 - 1 + r + H) % H;
+        const uint4 v = a.X[(size_t(n * H + y) * W + x) * CC + cc];
+        uint4* row = Xs + size_t(cc) * PS + r * W2;
+        row[x + 1] = v;
+        if (x == W - 1) row[0] = v;
+        if (x == 0) row[W + 1] = v;
+    }
+    for (int e = tid; e < 9 * CC * COUT; e += NT) Wt[e] = a.Wb[e];
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (tid == 0) {
+        constexpr uint32_t idesc = tc::idesc_bf16_f32(64, COUT);
+        const uint32_t xb = tc::smem_addr(Xs), wb = tc::smem_addr(Wt);
+        const uint32_t lbo_a = uint32_t(PS) * 16, lbo_b = COUT * 16;
+        for (int j = 0; j < 4; ++j) {  // tile j: row j / TPR, pixels (j % TPR) * 64 ..
+            const int r = j / TPR, x0 = (j % TPR) * 64;
+            const uint32_t d = tmem + (uint32_t(16 * (j & 1)) << 16) + (j >> 1) * COUT;
+            for (int sh = 0; sh < 9; ++sh) {
+                const int ky = sh / 3, kx = sh % 3;
+                for (int s = 0; s < CIN / 16; ++s) {
+                    const uint32_t aa = xb + ((2 * s) * PS + (r + ky) * W2 + x0 + kx) * 16;
+                    const uint32_t ba = wb + (sh * CC + 2 * s) * COUT * 16;
+                    tc::mma_bf16(d, tc::smem_desc(aa, lbo_a, 128), tc::smem_desc(ba, lbo_b, 128), idesc, (sh | s) != 0);
+                }
+            }
+        }
+        tc::mma_commit(bar);
+    }
+    const bool ok = tc::mbar_wait_bounded(bar, 0, a.err);
+    tc::fence_after_sync();
+    if (ok) {
+        for (int cs = 0; cs < 2; ++cs) {  // column set cs: tiles 2cs (lanes 0-15) and 2cs+1 (lanes 16-31)
+            float acc[32];
+            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + cs * COUT;
+            if constexpr (COUT == 32) tc::tmem_ld_32x32(taddr, acc);
+            else tc::tmem_ld_32x16(taddr, acc);
+            const int j = 2 * cs + (lane >> 4);
+            const int r = j / TPR, x = (j % TPR) * 64 + warp * 16 + (lane & 15);
+            const size_t gp = size_t(n * H + y0 + r) * W + x;
+            if constexpr (MODE == FVNET_CONV_HIDDEN) {
+                float z[COUT], g[COUT];
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) {
+                    z[c] = acc[c] + a.bias[c];
+                    g[c] = gelu_tanh(z[c]);
+                }
+                uint4* Zo = reinterpret_cast<uint4*>(a.Z + gp * COUT);
+                uint4* Ao = reinterpret_cast<uint4*>(a.A + gp * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) {
+                    Zo[q] = pack8(z + 8 * q);
+                    Ao[q] = pack8(g + 8 * q);
+                }
+            } else if constexpr (MODE == FVNET_CONV_OUTPUT) {
+                float4 o = make_float4(acc[0] + a.bias[0], acc[1] + a.bias[1], acc[2] + a.bias[2], acc[3] + a.bias[3]);
+                reinterpret_cast<float4*>(a.out4)[gp] = o;
+            } else {
+                float d[COUT];
+                const uint4* Zp = reinterpret_cast<const uint4*>(a.Zprev + gp * COUT);
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) {
+                    const uint4 u = Zp[q];
+                    const __nv_bfloat16* zb = reinterpret_cast<const __nv_bfloat16*>(&u);
+#pragma unroll
+                    for (int jj = 0; jj < 8; ++jj) {
+                        const float gz = (MODE == FVNET_CONV_BWD_GELU) ? gelu_tanh_grad(__bfloat162float(zb[jj])) : 1.0f;
+                        d[8 * q + jj] = acc[8 * q + jj] * gz;
                     }
                 }
                 uint4* Ao = reinterpret_cast<uint4*>(a.A + gp * COUT);
@@ -432,6 +559,17 @@ __global__ void pack_weights_kernel(const float* __restrict__ Wc, int cout, int 
 
 template <int CIN, int COUT, int MODE>
 int launch_conv(const ConvArgs& a, cudaStream_t st) {
+    if (a.W >= 64 && getenv("FVNET_CONV_COPIES") == nullptr) {  // one staged copy (FVNET_CONV_COPIES: three)
+        static bool rattr = false;
+        if (!rattr) {  // the limit for the largest image width served (W = 256)
+            if (cudaFuncSetAttribute(conv3x3_rows_kernel<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)rows_smem_bytes(CIN, COUT, 256)) != cudaSuccess)
+                return fv_internal_set_error(FVNET_ERR_CUDA, "fvnet: smem attribute");
+            rattr = true;
+        }
+        conv3x3_rows_kernel<CIN, COUT, MODE><<<dim3(a.H / (256 / a.W), a.B), NT, rows_smem_bytes(CIN, COUT, a.W), st>>>(a);
+        return FVNET_OK;
+    }
     const size_t smem = conv_smem_bytes(CIN, COUT, a.W);
     static bool attr = false;
     if (!attr) {  // the limit for the largest image width served (W = 256)

@@ -88,7 +88,9 @@ def test_rollout_metrics_match_the_reference_formulas(cuda_ok):
         np.testing.assert_allclose(g_rmse[ok], rmse[ok], rtol=1e-12, atol=0)
         okd = np.isfinite(drift)
         assert (np.isfinite(g_drift) == okd).all()
-        np.testing.assert_allclose(g_drift[okd], drift[okd], rtol=1e-9, atol=1e-15)
+        # the totals agree to roundoff, so the drift is a difference of two nearly equal sums of 4096
+        # terms whose last bits depend on the summation order (numpy pairwise, torch tree): ~1e-13
+        np.testing.assert_allclose(g_drift[okd], drift[okd], rtol=1e-9, atol=1e-12)
         assert (got["bad_cells"].cpu().numpy() == bad).all()
     assert int(pa.rollout_metrics(pred[0], truth[0], std)["bad_cells"].sum()) == 2
     assert int(pa.rollout_metrics(pred[1], truth[1], std)["bad_cells"].sum()) == 1
