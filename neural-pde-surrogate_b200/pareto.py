@@ -67,6 +67,22 @@ def truth_frames(items, n, coarse, frames, sizes, log=print):
     return torch.stack(out), {m: torch.stack(v).contiguous() for m, v in first.items()}
 
 
+def initial_frames(items, n, sizes):
+    """{m: (B, m, m, 4)} first frames of trajectories that start at t = 0 (Riemann, blast): their
+    n^2 initial conditions block-averaged to each size m (no fine solve needed)."""
+    import torch
+    ic = importlib.import_module(f"{PKG}.ic")
+    out = {m: [] for m in sizes}
+    for fam, idx in items:
+        rho, u, v, p, _, params = ic.sample(fam, idx, n)
+        if float(params.get("t_start", 0.0)) != 0.0:
+            raise ValueError(f"{fam} {idx} starts at t > 0: its first frame needs a fine solve")
+        U = torch.from_numpy(ic.to_conserved(rho, u, v, p)).cuda()[None]
+        for m in sizes:
+            out[m].append(block_avg(U, n // m)[0])
+    return {m: torch.stack(v).contiguous() for m, v in out.items()}
+
+
 def l1_density(U, T):
     """sum |rho - rho_true| dA per sample on the unit box, U and T (B, c, c, 4)."""
     c = U.shape[1]
@@ -108,7 +124,9 @@ def rollout_metrics(pred, true, std):
 
 
 def run_plain(first, n, coarse, frames, truth, families=None):
-    """All test trajectories at n^2 in one fv_ensemble; errors on the coarse grid."""
+    """All test trajectories at n^2 in one fv_ensemble; errors on the coarse grid.  The batch `first`
+    may hold more trajectories than `truth`: all are advanced and timed, the errors and drifts are
+    those of the first truth.shape[0]."""
     import torch
     fv = importlib.import_module(PKG)
     Ensemble = importlib.import_module(f"{PKG}.ensemble").Ensemble
@@ -131,7 +149,7 @@ def run_plain(first, n, coarse, frames, truth, families=None):
         ms += e0.elapsed_time(e1)
         status |= st
         ens.get_all(U)
-        l1.append(l1_density(block_avg(U, n // coarse), truth[:, k]))
+        l1.append(l1_density(block_avg(U[:truth.shape[0]], n // coarse), truth[:, k]))
     L1 = torch.stack(l1, dim=1)
     return {"method": "plain", "n": n, "L1_final": float(L1[:, -1].mean()), "L1_mean": float(L1.mean()),
             "L1_final_by_family": by_family(L1, families),
@@ -143,7 +161,8 @@ def run_plain(first, n, coarse, frames, truth, families=None):
 def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, families=None):
     """mode: positivity rule of the correction ('strict': a step that would go non-physical is the plain
     coarse step; 'scale': the largest physical fraction of the correction).  gain: a fixed factor on
-    every correction (1 = as trained)."""
+    every correction (1 = as trained).  As in run_plain, errors are those of the first
+    truth.shape[0] trajectories of the (timed) batch."""
     import torch
     corr = importlib.import_module(f"{PKG}.correction")
     z = np.load(model)
@@ -182,7 +201,7 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, fami
         fallbacks += int(fb.sum())
         theta.append(float(net.theta.mean()))
         x.copy_(Un)
-        l1.append(l1_density(x, truth[:, k]))
+        l1.append(l1_density(x[:truth.shape[0]], truth[:, k]))
     L1 = torch.stack(l1, dim=1)
     return {"method": f"hybrid-{mode}" + (f"-g{gain:g}" if gain != 1.0 else ""), "n": coarse, "gain": gain,
             "L1_final_by_family": by_family(L1, families), "L1_final": float(L1[:, -1].mean()), "L1_mean": float(L1.mean()),
