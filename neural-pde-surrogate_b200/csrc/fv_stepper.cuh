@@ -4,8 +4,8 @@
 // tiles of a stage finish at different times while the SMs that finished first sit idle, and the
 // next stage starts only when the whole grid is done.  Here a grid of (SMs x resident CTAs) CTAs
 // stays resident and pulls work items from one queue in a fixed order:
-//     item k  ->  step s = s0 + k / (2T), stage 1 if k mod 2T < T else stage 2, tile k mod T
-// (T tiles).  An item waits only for what it reads or overwrites, never for the whole grid:
+//     item k  ->  step s = s0 + k / (2T), stage 1 if k mod 2T < T else stage 2, a tile
+// (T tiles, visited in row-major order rotated by one tile row per stage).  An item waits only for what it reads or overwrites, never for the whole grid:
 //   * stage 1 of (s, t) reads U^s, W^s of t and its halo and overwrites U1, W1 of t, which stage 2
 //     of step s-1 read: it waits until stage 2 of step s-1 has finished on t's neighbours
 //     (flag2[n] >= s for every n in the tile's dependency list: the tiles its halo box maps to,
@@ -193,10 +193,14 @@ __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* 
         unsigned long long k = 0;
         if (lane == 0) k = atomicAdd(&c->queue, 1ull);
         k = __shfl_sync(0xffffffffu, k, 0);
-        const long long step = s0 + (long long)(k / (unsigned long long)(2 * T));
-        const long long r = (long long)(k % (unsigned long long)(2 * T));
-        const int stage = r < T ? 1 : 2;
-        const int tile = int(stage == 1 ? r : r - T);
+        // stage block b = k / T (step s0 + b/2, stage 1 + b%2); each block visits the tiles in row-major
+        // order starting one tile row further than the block before it, so that a block's first rows
+        // depend only on the first rows of the block before it (never on its last rows through a
+        // periodic wrap)
+        const long long b = (long long)(k / (unsigned long long)T);
+        const long long step = s0 + b / 2;
+        const int stage = int(b & 1) + 1;
+        const int tile = int(((long long)(k % (unsigned long long)T) + (b % st.nty) * st.ntx) % T);
         int go = step < s_end;
         double dt = 0.0;
         if (go && stage == 1) {

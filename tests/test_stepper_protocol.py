@@ -1,5 +1,5 @@
 """A discrete-event model of the persistent stepper's scheduling protocol (csrc/fv_stepper.cuh),
-run on the CPU: the queue order of items, stage 1's check of the previous step and its wait on the
+run on the CPU: the queue order of items (tile order rotated by one tile row per stage), stage 1's check of the previous step and its wait on the
 neighbours' stage-2 flags, its wait for the step's publication before its update, stage 2's waits,
 the last stage-2 item's publication of the next step, and the stop rule.  CTAs run with random
 durations.  The model must always terminate with the expected step count, every read must see the
@@ -47,6 +47,7 @@ def simulate(nx, ny, bcx, bcy, tx, ty, ctas, n_run, budget, seed, bad_at=None):
     dep = library_deps(nx, ny, bcx, bcy, tx, ty)
     reads = halo_reads(nx, ny, bcx, bcy, tx, ty)
     T = len(dep)
+    ntx, nty = -(-nx // tx), -(-ny // ty)
     s0 = 5
     flag1, flag2 = [s0] * T, [s0] * T
     W, W1 = [s0] * T, [None] * T            # the step whose state / stage-1 output each tile holds
@@ -70,8 +71,8 @@ def simulate(nx, ny, bcx, bcy, tx, ty, ctas, n_run, budget, seed, bad_at=None):
         while True:
             k = ctl["queue"]
             ctl["queue"] += 1
-            step, r = s0 + k // (2 * T), k % (2 * T)
-            stage, tile = (1, r) if r < T else (2, r - T)
+            blk = k // T  # stage block: step s0 + blk // 2, stage 1 + blk % 2, tile order rotated by blk rows
+            step, stage, tile = s0 + blk // 2, 1 + blk % 2, (k % T + (blk % nty) * ntx) % T
             if step >= s0 + budget:
                 return
             if stage == 1:
