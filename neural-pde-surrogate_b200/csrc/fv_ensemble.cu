@@ -205,8 +205,7 @@ int build_graph(fv_ensemble* e) {
 cudaError_t enqueue_batch(fv_ensemble* e);
 
 // The many-grid stepper's tables (first use): member m's tiles are entries base_m.. of the flags and
-// dependency lists, and CTA b starts on the member holding tile b * total / grid (largest members get
-// the most CTAs).
+// dependency lists, and the CTAs start on the members in proportion to their work.
 int prepare_stepper(fv_ensemble* e) {
     e->multi = multi_kernel(e->flux, e->lim);
     EN_CUDA(cudaFuncSetAttribute((const void*)e->multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
@@ -230,10 +229,15 @@ int prepare_stepper(fv_ensemble* e) {
     }
     const int T = (int)off.size() - 1;
     e->total_tiles = T;
+    // first member of every CTA, in proportion to the members' work: tiles x steps, and a member's
+    // steps to a given time grow with its resolution (CFL), so the weight is tiles x nx
+    std::vector<double> cum(e->count + 1, 0.0);
+    for (int m = 0; m < e->count; ++m)
+        cum[m + 1] = cum[m] + double(st[m].ntx) * st[m].nty * double(e->h_members[m].nx);
     std::vector<int> first(e->sgrid);
     for (int b = 0, m = 0; b < e->sgrid; ++b) {
-        const long long tile = (long long)b * T / e->sgrid;
-        while (m + 1 < e->count && base[m + 1] <= tile) ++m;
+        const double w = (b + 0.5) * cum[e->count] / e->sgrid;
+        while (m + 1 < e->count && cum[m + 1] <= w) ++m;
         first[b] = m;
     }
     const size_t bytes = 2 * size_t(T) * sizeof(unsigned) + (off.size() + idx.size() + first.size()) * sizeof(int) +
