@@ -448,7 +448,8 @@ def hybrid_leg(n_riemann=6, n_blast=6, n_kh=4, batch=128, frames=100, truth_n=10
     plains = [pareto.run_plain(first[n], n, coarse, frames, truth, fams) for n in plain]
     horizons = sorted({h for h in (5, 10, 20, 40, frames) if h <= frames})
     eq = pareto.equal_error(hyb, plains, horizons)
-    keep = ("L1_final", "L1_mean", "L1_final_by_family", "ms_per_traj", "drift_mass", "drift_energy")
+    keep = ("L1_final", "L1_mean", "L1_final_by_family", "ms_per_traj", "drift_mass", "drift_energy",
+            "substeps_mean_per_frame", "substeps_of_slowest_per_frame_mean", "substeps_max_per_frame")
     wins = {h: bool(r["plain_n"] and r["plain_n"] > coarse and r["speedup"] > 1.0) for h, r in eq.items()}
     return {"sample": f"errors: {n_riemann} Riemann + {n_blast} blast + {n_kh} Kelvin-Helmholtz held-out initial "
                       f"conditions (indices 200000+), {frames} frames of 0.005; times: per trajectory of a "

@@ -2,10 +2,13 @@
 //
 // The per-stage kernels (fv_kernels.cuh) launch twice per step, and every launch drains: the last
 // tiles of a stage finish at different times while the SMs that finished first sit idle, and the
-// next stage starts only when the whole grid is done.  Here a grid of (SMs x resident CTAs) CTAs
-// stays resident and pulls work items from one queue in a fixed order:
+// next stage starts only when the whole grid is done.  Here a grid of G = (SMs x resident CTAs) CTAs
+// stays resident and runs work items in a fixed order:
 //     item k  ->  step s = s0 + k / (2T), stage 1 if k mod 2T < T else stage 2, a tile
-// (T tiles, visited in row-major order rotated by one tile row per stage).  An item waits only for what it reads or overwrites, never for the whole grid:
+// (T tiles, visited in row-major order rotated by one tile row per stage).  CTA b runs items
+// b, b + G, b + 2G, ... in that order (an ensemble's members share one queue each instead, whose
+// items the CTAs claim with an atomic counter).  An item waits only for what it reads or
+// overwrites, never for the whole grid:
 //   * stage 1 of (s, t) reads U^s, W^s of t and its halo and overwrites U1, W1 of t, which stage 2
 //     of step s-1 read: it waits until stage 2 of step s-1 has finished on t's neighbours
 //     (flag2[n] >= s for every n in the tile's dependency list: the tiles its halo box maps to,
@@ -17,8 +20,11 @@
 //     only before its update (P4); stage 2 waits before it starts.  The last stage-2 item of step s
 //     publishes step s + 1 (publish_step), so the next step's first tiles overlap the current step's
 //     last ones instead of waiting for a drained grid.
-// Items wait only on items earlier in the queue, all CTAs are co-resident (cooperative launch), so
-// every wait ends; each is bounded in time all the same (FV_ERR_TIMEOUT, no hang).  The arithmetic
+// Every wait ends: an item waits only on items earlier in the order, every CTA runs its items in
+// increasing order and all CTAs are co-resident (cooperative launch), so the earliest unfinished
+// item is always the one its CTA is running, with every input finished.  Each wait is bounded in
+// time all the same (FV_ERR_TIMEOUT, no hang).  An item's completion (flag release, publication)
+// runs in one thread while the CTA's next item waits for its inputs and never waits itself.  The arithmetic
 // is tile_body's, so results are bit-identical to the per-stage kernels and to the reference.
 //
 // Memory ordering: a finished item's stores are published by one release store of its flag after
@@ -171,18 +177,87 @@ static __global__ void stepper_begin_kernel(const GridDesc g, StepperTiles st, l
     if (blockIdx.x == 0 && threadIdx.x == 0) begin_grid(g, nsteps);
 }
 
-// Claims the next item of grid g's queue, waits for its inputs (warp 0), and runs it.  Returns false
-// when the grid has no more items to run in this launch (past its last step, the loop has reached
-// t_next, a bad cell, or a timeout), true after running one.  Called by every thread of the CTA; the
-// mbarrier s.bar (when tm is used) is initialised and `phase` tracks it.
-template <int FLUX, int LIM, int TX, int TY, int NT>
-__device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* tm, const StepperTiles& st,
-                                             TileSmem<TX, TY>& s, uint32_t& phase) {
-    __shared__ double s_dt;
-    __shared__ int s_go, s_tile, s_stage;
-    __shared__ long long s_step;
+// Per-CTA state of the item loop, in shared memory.  The current item (step, stage, tile, dt, go) is
+// written by lane 0 of warp 0 before the claim barrier.  The previous item's completion -- its
+// block-reduced wave speeds and first bad cell, its flag release, and for stage 2 the step count
+// and possibly the publication of the step -- runs in thread 32 (warp 1) while warp 0 claims and
+// waits for the next item, so that completion and the next wait overlap instead of adding up.
+struct StepperSlot {
+    double dt;
+    long long step;
+    int go, tile, stage;
+    unsigned long long next;  // the CTA's next item when items are assigned statically
+    double red_sx, red_sy;    // the previous stage-2 item's block maxima, its first bad cell
+    int red_bad;
+    long long prev_step;      // the previous item (prev_stage 0: none)
+    int prev_stage, prev_tile;
+};
+constexpr int kTailThread = 32;
+
+// Completion of item (step, stage, tile) of grid g, by one thread, after a CTA barrier that follows
+// every store of the item: the stage-2 reduction into the next step's slot, then the release of the
+// tile's flag; for stage 2 the count of finished stage-2 items, and by the last one of the step its
+// publication.
+__device__ __forceinline__ void item_tail(const GridDesc& g, const StepperTiles& st, const StepperSlot& sl) {
     FvCtrl* c = g.ctrl;
-    // ---- claim the next item and wait for its inputs (warp 0) ----
+    const long long step = sl.prev_step;
+    const int tile = st.base + sl.prev_tile;
+    fence_proxy_async_global();
+    if (sl.prev_stage == 1) {
+        __threadfence();
+        st_release(st.flag1 + tile, unsigned(step + 1));
+        return;
+    }
+    const int par = int((step + 1) & 1);
+    if (sl.red_sx > 0.0) atomicMax(&c->sxy[par][0], (unsigned long long)__double_as_longlong(sl.red_sx));
+    if (sl.red_sy > 0.0) atomicMax(&c->sxy[par][1], (unsigned long long)__double_as_longlong(sl.red_sy));
+    if (sl.red_bad != INT_MAX) atomicMin(&c->bad[par], sl.red_bad);
+    __threadfence();
+    st_release(st.flag2 + tile, unsigned(step + 1));
+    const unsigned long long n = atomicAdd(&c->done2, 1ull) + 1ull;
+    const unsigned long long T = (unsigned long long)st.ntx * st.nty;
+    if (n == (unsigned long long)(step - c->s0 + 1) * T) {
+        __threadfence();  // every other item's reduction atomics precede their counts
+        publish_step(c, g, step);
+    }
+}
+
+// Block maxima of the wave speeds and minimum bad index into sl.red_* (thread 0 writes them); the
+// per-stage kernels' reduce_wave_speeds without its global atomics, which item_tail issues.
+template <int NT>
+__device__ __forceinline__ void block_wave_speeds(double sx, double sy, int bad, StepperSlot& sl) {
+    constexpr int NW = NT / 32;
+    __shared__ double rsx[NW], rsy[NW];
+    __shared__ int rbad[NW];
+    sx = warp_max(sx);
+    sy = warp_max(sy);
+    bad = warp_min_int(bad);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { rsx[w] = sx; rsy[w] = sy; rbad[w] = bad; }
+    __syncthreads();
+    if (w == 0) {
+        sx = l < NW ? rsx[l] : 0.0;
+        sy = l < NW ? rsy[l] : 0.0;
+        bad = l < NW ? rbad[l] : INT_MAX;
+        sx = warp_max(sx);
+        sy = warp_max(sy);
+        bad = warp_min_int(bad);
+        if (l == 0) { sl.red_sx = sx; sl.red_sy = sy; sl.red_bad = bad; }
+    }
+}
+
+// Runs grid g's next item: warp 0 takes it (STATIC: the CTA's own sequence blockIdx.x + i gridDim.x;
+// else the grid's shared queue) and waits for its inputs, while thread 32 completes the previous
+// item; then the CTA runs the tile body.  Returns false when the grid has no more items to run in
+// this launch (past its last step, the loop has reached t_next, a bad cell, or a timeout), true after
+// running one.  Called by every thread of the CTA; the mbarrier s.bar (when tm is used) is
+// initialised and `phase` tracks it.  sl.prev_stage must be 0 on the first call for a grid, and
+// sl.next the CTA's first item when STATIC.
+template <int FLUX, int LIM, int TX, int TY, int NT, bool STATIC>
+__device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* tm, const StepperTiles& st,
+                                             TileSmem<TX, TY>& s, uint32_t& phase, StepperSlot& sl) {
+    FvCtrl* c = g.ctrl;
+    // ---- take the next item and wait for its inputs (warp 0); complete the previous one (thread 32) ----
     // (launch constants are re-read here rather than kept in registers across the tile body)
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x & 31;
@@ -191,7 +266,14 @@ __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* 
         const bool loop_mode = c->mode == MODE_LOOP;
         const double t_next = c->t_next;
         unsigned long long k = 0;
-        if (lane == 0) k = atomicAdd(&c->queue, 1ull);
+        if (lane == 0) {
+            if constexpr (STATIC) {
+                k = sl.next;
+                sl.next = k + gridDim.x;
+            } else {
+                k = atomicAdd(&c->queue, 1ull);
+            }
+        }
         k = __shfl_sync(0xffffffffu, k, 0);
         // stage block b = k / T (step s0 + b/2, stage 1 + b%2); each block visits the tiles in row-major
         // order starting one tile row further than the block before it, so that a block's first rows
@@ -228,74 +310,72 @@ __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* 
         }
         if (lane == 0) {
             if (go) fence_proxy_async_global();  // before this thread issues the tile's TMA load
-            s_go = go;
-            s_step = step;
-            s_stage = stage;
-            s_tile = tile;
-            s_dt = dt;
+            sl.go = go;
+            sl.step = step;
+            sl.stage = stage;
+            sl.tile = tile;
+            sl.dt = dt;
         }
+    } else if (threadIdx.x == kTailThread && sl.prev_stage != 0) {
+        item_tail(g, st, sl);
     }
     __syncthreads();
-    if (!s_go) return false;
-    const int tyi = s_tile / st.ntx, txi = s_tile - tyi * st.ntx;
+    if (threadIdx.x == kTailThread) {  // the item to complete next time, if it runs to its end
+        sl.prev_step = sl.step;
+        sl.prev_stage = sl.go ? sl.stage : 0;
+        sl.prev_tile = sl.tile;
+    }
+    if (!sl.go) return false;
+    const int tyi = sl.tile / st.ntx, txi = sl.tile - tyi * st.ntx;
     double sx = 0.0, sy = 0.0;
     int bad = INT_MAX;
     const int one = 1;
     auto ctl = []() {};
     bool done;
-    if (s_stage == 1) {
+    if (sl.stage == 1) {
         // stage 1 waits for its step's publication only before its update
         auto pre4 = [&]() -> bool {
             if (threadIdx.x == 0) {
-                const long long step = s_step;
+                const long long step = sl.step;
                 const bool ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
-                s_dt = __ldcg(&c->sdt[step & 1]);
-                s_go = ok;
+                sl.dt = __ldcg(&c->sdt[step & 1]);
+                sl.go = ok;
             }
             __syncthreads();
-            return s_go != 0;
+            return sl.go != 0;
         };
         done = tile_body<FLUX, LIM, 1, TX, TY, NT, decltype(ctl), decltype(pre4), true>(
-            g, tm, phase, txi * TX, tyi * TY, s_dt, one, ctl, s, sx, sy, bad, pre4);
+            g, tm, phase, txi * TX, tyi * TY, sl.dt, one, ctl, s, sx, sy, bad, pre4);
     } else {
-        done = tile_body<FLUX, LIM, 2, TX, TY, NT, decltype(ctl), NoPre4, true>(g, tm, phase, txi * TX, tyi * TY, s_dt,
+        done = tile_body<FLUX, LIM, 2, TX, TY, NT, decltype(ctl), NoPre4, true>(g, tm, phase, txi * TX, tyi * TY, sl.dt,
                                                                                 one, ctl, s, sx, sy, bad);
     }
-    if (!done) return false;  // the step does not run (a bad cell or a timeout stopped the grid)
-    if (s_stage == 2) reduce_wave_speeds<NT>(sx, sy, bad, c, int((s_step + 1) & 1));  // ends with no barrier
-    __syncthreads();  // every store of this item precedes the flag's release
-    if (threadIdx.x == 0) {
-        const long long step = s_step;
-        const int tile = st.base + s_tile;
-        fence_proxy_async_global();
-        __threadfence();
-        if (s_stage == 1) {
-            st_release(st.flag1 + tile, unsigned(step + 1));
-        } else {
-            st_release(st.flag2 + tile, unsigned(step + 1));
-            const unsigned long long n = atomicAdd(&c->done2, 1ull) + 1ull;
-            const unsigned long long T = (unsigned long long)st.ntx * st.nty;
-            if (n == (unsigned long long)(step - c->s0 + 1) * T) {
-                __threadfence();  // every other item's reduction atomics precede their counts
-                publish_step(c, g, step);
-            }
-        }
+    if (!done) {  // the step does not run (a bad cell or a timeout stopped the grid): nothing to complete
+        if (threadIdx.x == kTailThread) sl.prev_stage = 0;
+        return false;
     }
+    if (sl.stage == 2) block_wave_speeds<NT>(sx, sy, bad, sl);  // ends with no barrier
+    __syncthreads();  // every store of this item precedes its completion (the next call's item_tail)
     return true;
 }
 
-// One grid: every CTA runs items of the grid's queue until it has none left.
+// One grid: CTA b runs items b, b + G, b + 2G, ... (G CTAs) in order until it has none left.
 template <int FLUX, int LIM, int TX, int TY, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stepper_kernel(const GridDesc g, const __grid_constant__ TileMaps tm,
                                                            const StepperTiles st) {
     extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destination: 128-byte aligned
     auto& s = *reinterpret_cast<TileSmem<TX, TY>*>(smem_raw);
-    if (tm.use && threadIdx.x == 0) {
-        tc::mbar_init(&s.bar, 1);
-        tc::fence_mbar_init();
+    __shared__ StepperSlot sl;
+    if (threadIdx.x == 0) {
+        if (tm.use) {
+            tc::mbar_init(&s.bar, 1);
+            tc::fence_mbar_init();
+        }
+        sl.next = blockIdx.x;
     }
+    if (threadIdx.x == kTailThread) sl.prev_stage = 0;
     uint32_t phase = 0;
-    while (stepper_item<FLUX, LIM, TX, TY, NT>(g, &tm, st, s, phase)) {
+    while (stepper_item<FLUX, LIM, TX, TY, NT, true>(g, &tm, st, s, phase, sl)) {
     }
 }
 
@@ -316,6 +396,8 @@ __global__ void __launch_bounds__(NT, MINB) multi_stepper_kernel(const GridDesc*
     __shared__ int s_member;
     __shared__ GridDesc s_g;      // the current member's descriptors, read from shared memory as needed
     __shared__ StepperTiles s_st;
+    __shared__ StepperSlot sl;
+    if (threadIdx.x == kTailThread) sl.prev_stage = 0;
     if (threadIdx.x == 0) {
         if (maps) {
             tc::mbar_init(&s.bar, 1);
@@ -332,7 +414,8 @@ __global__ void __launch_bounds__(NT, MINB) multi_stepper_kernel(const GridDesc*
     for (;;) {
         const int m = s_member;
         if (m < 0) return;
-        if (!stepper_item<FLUX, LIM, TX, TY, NT>(s_g, maps ? maps + m : nullptr, s_st, s, phase)) {
+        // a false return leaves nothing to complete (sl.prev_stage 0), so the member may change
+        if (!stepper_item<FLUX, LIM, TX, TY, NT, false>(s_g, maps ? maps + m : nullptr, s_st, s, phase, sl)) {
             if (threadIdx.x == 0) {
                 atomicExch(member_done + m, 1u);
                 const unsigned start = atomicAdd(cursor, 1u);

@@ -141,10 +141,13 @@ def run_plain(first, n, coarse, frames, truth, families=None):
     l1, ms = [], 0.0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     status = np.zeros(B, np.int32)
+    prev, substeps = np.zeros(B, np.int64), []
     for k in range(1, frames + 1):
         e0.record()
-        _, _, st = ens.advance_to(DT_FRAME * k, raise_on_nonphysical=False)
+        _, steps, st = ens.advance_to(DT_FRAME * k, raise_on_nonphysical=False)
         e1.record()
+        substeps.append((int((steps - prev).max()), float((steps - prev).mean())))
+        prev = steps
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
         status |= st
@@ -155,7 +158,10 @@ def run_plain(first, n, coarse, frames, truth, families=None):
             "L1_final_by_family": by_family(L1, families),
             "L1_per_frame": [round(float(v), 5) for v in L1.mean(dim=0)],
             "ms_per_traj": ms / B, "drift_mass": float(drift(U, first)[:, 0].abs().max()),
-            "drift_energy": float(drift(U, first)[:, 3].abs().max()), "failed": int((status != 0).sum())}
+            "drift_energy": float(drift(U, first)[:, 3].abs().max()), "failed": int((status != 0).sum()),
+            "substeps_max_per_frame": max(m for m, _ in substeps),
+            "substeps_mean_per_frame": float(np.mean([a for _, a in substeps])),
+            "substeps_of_slowest_per_frame_mean": float(np.mean([m for m, _ in substeps]))}
 
 
 def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, families=None):
@@ -178,10 +184,12 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, fami
     corr.hybrid_step(net, cs, x.clone(), 1e-9, stats, dscale, Uc, Un, fb, mode)  # warm-up (kernel loading)
     torch.cuda.synchronize()
     l1, ms, fallbacks, theta, retried, failed = [], 0.0, 0, [], 0, 0
+    substeps = []  # per frame: the coarse CFL sub-steps of the slowest and of the mean trajectory
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for k in range(1, frames + 1):
         e0.record()
-        _, status = corr.hybrid_step(net, cs, x, DT_FRAME, stats, dscale, Uc, Un, fb, mode)
+        steps, status = corr.hybrid_step(net, cs, x, DT_FRAME, stats, dscale, Uc, Un, fb, mode)
+        substeps.append((int(np.max(steps)), float(np.mean(steps))))
         bad = np.nonzero(status)[0]
         if len(bad):
             # the coarse solver cannot advance these corrected states: drop the previous frame's
@@ -208,7 +216,10 @@ def run_hybrid(model, first, coarse, frames, truth, mode="scale", gain=1.0, fami
             "L1_per_frame": [round(float(v), 5) for v in L1.mean(dim=0)], "mean_theta": float(np.mean(theta)),
             "ms_per_traj": ms / B, "drift_mass": float(drift(x, first)[:, 0].abs().max()),
             "drift_energy": float(drift(x, first)[:, 3].abs().max()), "fallback_steps": fallbacks,
-            "coarse_retries": retried, "failed": failed}
+            "coarse_retries": retried, "failed": failed,
+            "substeps_max_per_frame": max(m for m, _ in substeps),
+            "substeps_mean_per_frame": float(np.mean([a for _, a in substeps])),
+            "substeps_of_slowest_per_frame_mean": float(np.mean([m for m, _ in substeps]))}
 
 
 def equal_error(hyb, plains, horizons):
