@@ -44,6 +44,22 @@ __device__ __forceinline__ Q4 ldg_q4(const Q4* p) {
 __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 
+// Magnitude tests from the exponent field (integer compares, which leave the FP64 pipe free):
+// mag_in<LO, HI>(x): 2^LO <= |x| < 2^HI; pos_in<LO, HI>(x): 2^LO <= x < 2^HI (x positive).  Zeros,
+// subnormals, infinities and NaN fail both.  The high word of |x| orders like |x| on exponent
+// boundaries, and a negative x has the sign bit set, which puts it above the range as unsigned.
+template <int LO, int HI>
+__device__ __forceinline__ bool mag_in(double x) {
+    static_assert(LO < HI && 1023 + LO > 0 && 1023 + HI < 2047, "exponent range");
+    const unsigned h = unsigned(__double2hiint(x)) & 0x7fffffffu;
+    return h - unsigned((1023 + LO) << 20) < unsigned((HI - LO) << 20);
+}
+template <int LO, int HI>
+__device__ __forceinline__ bool pos_in(double x) {
+    static_assert(LO < HI && 1023 + LO > 0 && 1023 + HI < 2047, "exponent range");
+    return unsigned(__double2hiint(x)) - unsigned((1023 + LO) << 20) < unsigned((HI - LO) << 20);
+}
+
 // ---- two correctly rounded divisions for special operands ------------------------------------
 // Both return exactly the IEEE round-to-nearest quotient (what `/` returns) for every finite input;
 // outside the ranges where their reasoning holds they fall back to `/`.
@@ -55,8 +71,7 @@ __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b 
 // within 0.9 ulp of a/b and the theorem applies.
 constexpr double Y_GM1 = 1.0 / GM1;  // RN(1/(GAMMA-1)) = 2.5000000000000004
 __device__ __forceinline__ double div_gm1(double p) {
-    const double a = fabs(p);
-    if (!(a > 0x1p-900 && a < 0x1p+900)) return p / GM1;  // zero, subnormal, huge, inf, NaN
+    if (!mag_in<-899, 900>(p)) return p / GM1;  // zero, subnormal, huge, inf, NaN
     const double q0 = p * Y_GM1;
     const double r = fma(-q0, GM1, p);
     return fma(r, Y_GM1, q0);
@@ -71,11 +86,10 @@ __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 // y + y(1 - b y), q0 = a y, and Markstein's correction q0 + (a - q0 b) y (the method cited above).
 // Emulated on a CPU with seeds of relative error up to 2^-20 this gave the correctly rounded
 // quotient for all of 2e7 random operand pairs, and at most 1 ulp from 2^-14 seeds.  Operands
-// outside 2^-500 < |a|, |b| < 2^500 take `/`: zeros (so that a signed zero keeps IEEE's sign),
+// outside 2^-499 <= |a|, |b| < 2^500 take `/`: zeros (so that a signed zero keeps IEEE's sign),
 // infinities, NaN, and the extremes whose quotient could be subnormal or overflow.
 __device__ __forceinline__ double fdiv(double a, double b) {
-    const double mb = fabs(b), ma = fabs(a);
-    if (!(mb > 0x1p-500 && mb < 0x1p+500 && ma > 0x1p-500 && ma < 0x1p+500)) return a / b;
+    if (!(mag_in<-499, 500>(a) && mag_in<-499, 500>(b))) return a / b;
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
     y = fma(y, fma(-b, y, 1.0), y);
@@ -83,9 +97,9 @@ __device__ __forceinline__ double fdiv(double a, double b) {
     return fma(fma(-q, b, a), y, q);
 }
 // 1/b for divisions that share a denominator: the same seed and two Newton-Raphson steps (a quotient
-// a * recip(b) is then within about 1.5 ulp); operands outside 2^-500 < |b| < 2^500 take `/`.
+// a * recip(b) is then within about 1.5 ulp); operands outside 2^-499 <= |b| < 2^500 take `/`.
 __device__ __forceinline__ double recip(double b) {
-    if (!(fabs(b) > 0x1p-500 && fabs(b) < 0x1p+500)) return 1.0 / b;
+    if (!mag_in<-499, 500>(b)) return 1.0 / b;
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
     y = fma(y, fma(-b, y, 1.0), y);
@@ -98,7 +112,7 @@ __device__ __forceinline__ double recip(double b) {
 // nonzero, non-NaN b (infinities included), which is a * copysign(1, b) exactly.  The general
 // division routine treats a zero numerator as a special case and runs ~3x slower on it.
 __device__ __forceinline__ double div_z(double a, double b) {
-    if (a == 0.0 && b != 0.0 && b == b) return a * copysign(1.0, b);
+    if ((__double_as_longlong(a) << 1) == 0 && b != 0.0 && b == b) return a * copysign(1.0, b);  // a = +-0
     return fdiv(a, b);
 }
 
@@ -110,17 +124,18 @@ __device__ __forceinline__ double div_z(double a, double b) {
 // 26(6), 2005), so the exact quotient is m/rho = u - e/rho, and |e/rho| <= 2^-53 |u| (1 + 2^-53) <
 // ulp(u).  Its correctly rounded value is u when |e/rho| < ulp(u)/2, else the neighbour of u on the
 // side of -e/rho.  No tie can occur: the exact quotient of two doubles is never halfway between two
-// doubles.  When u is a power of two the product is exact and e = 0.  The bound 2^-300 < rho, |u| <
+// doubles.  When u is a power of two the product is exact and e = 0.  The bound 2^-299 <= rho, |u| <
 // 2^300 keeps e, rho*ulp(u)/2 and rho*u normal; outside it (a zero, negative or extreme density, a
-// zero or extreme velocity) the division is done.
+// zero or extreme velocity) the division is done.  e is nonzero past the first test, so its sign
+// and u's compare as sign bits.
 __device__ __forceinline__ double div_back(double m, double rho, double u) {
-    const double au = fabs(u);
-    if (!(rho > 0x1p-300 && rho < 0x1p+300 && au > 0x1p-300 && au < 0x1p+300)) return div_z(m, rho);
+    if (!(pos_in<-299, 300>(rho) && mag_in<-299, 300>(u))) return div_z(m, rho);
     const double e = fma(rho, u, -m);
     const double half_ulp = __hiloint2double((__double2hiint(u) & 0x7ff00000) - (53 << 20), 0);  // 2^(k-53)
     if (fabs(e) < rho * half_ulp) return u;
     const long long bits = __double_as_longlong(u);
-    return __longlong_as_double(((e > 0.0) == (u > 0.0)) ? bits - 1 : bits + 1);  // toward zero if same sign
+    const bool same_sign = (__double2hiint(e) ^ __double2hiint(u)) >= 0;
+    return __longlong_as_double(same_sign ? bits - 1 : bits + 1);  // toward zero if same sign
 }
 
 // state2d.hpp:16-19 (p / (GAMMA - 1.0) through div_gm1: same bits, fewer instructions)

@@ -52,6 +52,12 @@ __device__ __forceinline__ void st_release(long long* p, long long v) {
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+// atomicAdd with release semantics at GPU scope; returns the old value.
+__device__ __forceinline__ unsigned long long atom_add_release(unsigned long long* p, unsigned long long v) {
+    unsigned long long old;
+    asm volatile("atom.release.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
 // Orders this thread's generic-proxy view of global memory with its asynchronous-proxy (TMA)
 // accesses: W and W1 are written by ordinary stores and read by TMA in the same launch.
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
@@ -123,36 +129,40 @@ __device__ __forceinline__ bool wait_flags(FvCtrl* c, const unsigned* flag, cons
 // The decisions are those of stage1_control, so a grid may alternate between the two paths.
 __device__ __forceinline__ void publish_step(FvCtrl* c, const GridDesc& g, long long j) {
     const int p1 = int((j + 1) & 1);
+    // every input first (independent loads, one round trip), then the decisions
     const double t1 = __ldcg(&c->t[p1]);
-    bool run = status_now(c) == 0 && j + 1 < c->s_end;
+    const int status = status_now(c), bad = __ldcg(&c->bad[p1]);
+    const double sx = __longlong_as_double((long long)__ldcg(&c->sxy[p1][0]));
+    const double sy = __longlong_as_double((long long)__ldcg(&c->sxy[p1][1]));
+    const long long s_end = c->s_end;
+    const int mode = c->mode;
+    const double t_next = c->t_next, dt_fixed = c->dt_fixed;
+    bool run = status == 0 && j + 1 < s_end;
     double dt = 0.0;
     if (run) {
-        if (c->mode == MODE_FIXED) {
-            dt = c->dt_fixed;
-        } else if (!(t1 < c->t_next)) {
+        if (mode == MODE_FIXED) {
+            dt = dt_fixed;
+        } else if (!(t1 < t_next)) {
             run = false;
-        } else if (__ldcg(&c->bad[p1]) != INT_MAX) {
+        } else if (bad != INT_MAX) {
             run = false;
-            c->bad_index = __ldcg(&c->bad[p1]);
+            c->bad_index = bad;
             c->status = 3;  // FV_ERR_NONPHYSICAL
         } else {
-            const double sx = __longlong_as_double((long long)__ldcg(&c->sxy[p1][0]));
-            const double sy = __longlong_as_double((long long)__ldcg(&c->sxy[p1][1]));
-            dt = smin(g.cfl / (sx / g.dx + sy / g.dy), c->t_next - t1);
+            dt = smin(g.cfl / (sx / g.dx + sy / g.dy), t_next - t1);
         }
     }
     c->srun[p1] = run ? 1 : 0;
     c->sdt[p1] = dt;
     if (!run) c->stop = j + 1;  // before the release below: a waiter that sees complete = j sees it
     if (run) {
-        c->t[p1 ^ 1] = (c->mode == MODE_FIXED) ? t1 : t1 + dt;  // fv_step does not advance the time
+        c->t[p1 ^ 1] = (mode == MODE_FIXED) ? t1 : t1 + dt;  // fv_step does not advance the time
         c->sxy[p1 ^ 1][0] = 0ull;
         c->sxy[p1 ^ 1][1] = 0ull;
         c->bad[p1 ^ 1] = INT_MAX;
     }
     c->step = j + 1;
-    __threadfence();
-    st_release(&c->complete, j);
+    st_release(&c->complete, j);  // release: every write above precedes it
 }
 
 // Launch prologue (one small grid before every stepper launch): the queue, the step range, every
@@ -178,52 +188,100 @@ static __global__ void stepper_begin_kernel(const GridDesc g, StepperTiles st, l
 }
 
 // Per-CTA state of the item loop, in shared memory.  The current item (step, stage, tile, dt, go) is
-// written by lane 0 of warp 0 before the claim barrier.  The previous item's completion -- its
-// block-reduced wave speeds and first bad cell, its flag release, and for stage 2 the step count
-// and possibly the publication of the step -- runs in thread 32 (warp 1) while warp 0 claims and
-// waits for the next item, so that completion and the next wait overlap instead of adding up.
+// written by lane 0 of warp 0 before the claim barrier.  The previous item's completion runs in two
+// threads while warp 0 claims and waits for the next item, so that completion and the next wait
+// overlap instead of adding up: thread 32 releases the tile's flag; thread 64, for a stage-2 item,
+// adds its block-reduced wave speeds and first bad cell into the next step's slot, counts the item
+// and, as the step's last, publishes the step.
 struct StepperSlot {
     double dt;
     long long step;
     int go, tile, stage;
-    unsigned long long next;  // the CTA's next item when items are assigned statically
-    double red_sx, red_sy;    // the previous stage-2 item's block maxima, its first bad cell
+    // the grid's launch constants (written by the prologue kernel), read once
+    long long s0, s_end;
+    double t_next;
+    int loop, T;
+    // STATIC item sequence: the next item is position r of stage block b (bm = b mod nty); the
+    // sequence advances by G = gridDim.x items, i.e. g_blocks blocks and g_rest positions
+    long long b;
+    int r, bm, g_blocks, g_rest;
+    // the last two publications this CTA saw, by the parity of the step j: whether step j + 1 runs,
+    // its dt and t_{j+2} (a publication never changes once made)
+    long long pub[2];
+    int pub_run[2];
+    double pub_dt[2], pub_t2[2];
+    double red_sx, red_sy;  // the previous stage-2 item's block maxima, its first bad cell
     int red_bad;
-    long long prev_step;      // the previous item (prev_stage 0: none)
+    long long prev_step;  // the previous item (prev_stage 0: none)
     int prev_stage, prev_tile;
 };
-constexpr int kTailThread = 32;
+constexpr int kFlagThread = 32, kCountThread = 64;
 
-// Completion of item (step, stage, tile) of grid g, by one thread, after a CTA barrier that follows
-// every store of the item: the stage-2 reduction into the next step's slot, then the release of the
-// tile's flag; for stage 2 the count of finished stage-2 items, and by the last one of the step its
-// publication.
-__device__ __forceinline__ void item_tail(const GridDesc& g, const StepperTiles& st, const StepperSlot& sl) {
+// Loads grid g's launch constants into the slot and resets its per-grid state; for STATIC items
+// also the CTA's first item (blockIdx.x).  One thread, followed by a CTA barrier.
+__device__ __forceinline__ void slot_begin(StepperSlot& sl, const GridDesc& g, const StepperTiles& st, bool is_static) {
+    const FvCtrl* c = g.ctrl;
+    sl.s0 = c->s0;
+    sl.s_end = c->s_end;
+    sl.t_next = c->t_next;
+    sl.loop = c->mode == MODE_LOOP;
+    sl.T = st.ntx * st.nty;
+    sl.pub[0] = sl.pub[1] = LLONG_MIN;
+    sl.prev_stage = 0;
+    if (is_static) {
+        const unsigned long long T = (unsigned long long)sl.T, G = gridDim.x;
+        sl.b = (long long)(blockIdx.x / T);
+        sl.r = int(blockIdx.x % T);
+        sl.bm = int(sl.b % st.nty);
+        sl.g_blocks = int(G / T);
+        sl.g_rest = int(G % T);
+    }
+}
+
+// Lane 0 of warp 0 / thread 0: has step `target` been published (waiting for it, bounded)?  Returns
+// the slot entry q (target's parity) whose pub_run[q] / pub_dt[q] / pub_t2[q] hold whether step
+// target + 1 runs, its dt and t_{target+2}, or -1 when it never will be (wait_complete).  A CTA asks
+// for the same publications for several items, so they are read from L2 once.  The global fields read
+// are the ones publish_step(target) wrote: the next write of their parity is publish_step(target + 2),
+// which needs the asking item to have finished.
+__device__ __forceinline__ int published(FvCtrl* c, StepperSlot& sl, long long target) {
+    const int q = int(target & 1);
+    if (sl.pub[q] == target) return q;
+    if (!wait_complete(c, target)) return -1;
+    const int p = int((target + 1) & 1);
+    sl.pub_run[q] = __ldcg(&c->srun[p]);
+    sl.pub_dt[q] = __ldcg(&c->sdt[p]);
+    sl.pub_t2[q] = __ldcg(&c->t[p ^ 1]);
+    sl.pub[q] = target;
+    return q;
+}
+
+// The previous item's completion, after the CTA barrier that follows its stores.  Thread 32: the
+// release of the tile's flag (cumulative over the CTA's stores through the barrier).  Thread 64, for
+// stage 2: the reduction into slot (step + 1) & 1, then the count (a release: the reduction precedes
+// it), and by the step's last item the publication (after an acquire fence: every other item's
+// reduction precedes its count, which precedes this one).
+__device__ __forceinline__ void release_flag(const StepperTiles& st, const StepperSlot& sl) {
+    fence_proxy_async_global();
+    unsigned* flag = (sl.prev_stage == 1) ? st.flag1 : st.flag2;
+    st_release(flag + st.base + sl.prev_tile, unsigned(sl.prev_step + 1));
+}
+__device__ __forceinline__ void count_stage2(const GridDesc& g, const StepperSlot& sl) {
     FvCtrl* c = g.ctrl;
     const long long step = sl.prev_step;
-    const int tile = st.base + sl.prev_tile;
-    fence_proxy_async_global();
-    if (sl.prev_stage == 1) {
-        __threadfence();
-        st_release(st.flag1 + tile, unsigned(step + 1));
-        return;
-    }
     const int par = int((step + 1) & 1);
     if (sl.red_sx > 0.0) atomicMax(&c->sxy[par][0], (unsigned long long)__double_as_longlong(sl.red_sx));
     if (sl.red_sy > 0.0) atomicMax(&c->sxy[par][1], (unsigned long long)__double_as_longlong(sl.red_sy));
     if (sl.red_bad != INT_MAX) atomicMin(&c->bad[par], sl.red_bad);
-    __threadfence();
-    st_release(st.flag2 + tile, unsigned(step + 1));
-    const unsigned long long n = atomicAdd(&c->done2, 1ull) + 1ull;
-    const unsigned long long T = (unsigned long long)st.ntx * st.nty;
-    if (n == (unsigned long long)(step - c->s0 + 1) * T) {
-        __threadfence();  // every other item's reduction atomics precede their counts
+    const unsigned long long n = atom_add_release(&c->done2, 1ull) + 1ull;
+    if (n == (unsigned long long)(step - sl.s0 + 1) * (unsigned long long)sl.T) {
+        __threadfence();
         publish_step(c, g, step);
     }
 }
 
 // Block maxima of the wave speeds and minimum bad index into sl.red_* (thread 0 writes them); the
-// per-stage kernels' reduce_wave_speeds without its global atomics, which item_tail issues.
+// per-stage kernels' reduce_wave_speeds without its global atomics, which count_stage2 issues.
 template <int NT>
 __device__ __forceinline__ void block_wave_speeds(double sx, double sy, int bad, StepperSlot& sl) {
     constexpr int NW = NT / 32;
@@ -247,63 +305,72 @@ __device__ __forceinline__ void block_wave_speeds(double sx, double sy, int bad,
 }
 
 // Runs grid g's next item: warp 0 takes it (STATIC: the CTA's own sequence blockIdx.x + i gridDim.x;
-// else the grid's shared queue) and waits for its inputs, while thread 32 completes the previous
-// item; then the CTA runs the tile body.  Returns false when the grid has no more items to run in
-// this launch (past its last step, the loop has reached t_next, a bad cell, or a timeout), true after
-// running one.  Called by every thread of the CTA; the mbarrier s.bar (when tm is used) is
-// initialised and `phase` tracks it.  sl.prev_stage must be 0 on the first call for a grid, and
-// sl.next the CTA's first item when STATIC.
+// else the grid's shared queue) and waits for its inputs, while threads 32 and 64 complete the
+// previous item; then the CTA runs the tile body.  Returns false when the grid has no more items to
+// run in this launch (past its last step, the loop has reached t_next, a bad cell, or a timeout),
+// true after running one.  Called by every thread of the CTA after slot_begin; the mbarrier s.bar
+// (when tm is used) is initialised and `phase` tracks it.
 template <int FLUX, int LIM, int TX, int TY, int NT, bool STATIC>
 __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* tm, const StepperTiles& st,
                                              TileSmem<TX, TY>& s, uint32_t& phase, StepperSlot& sl) {
+    static_assert(NT > kCountThread, "the completion threads must exist");
     FvCtrl* c = g.ctrl;
-    // ---- take the next item and wait for its inputs (warp 0); complete the previous one (thread 32) ----
-    // (launch constants are re-read here rather than kept in registers across the tile body)
+    // ---- take the next item and wait for its inputs (warp 0); complete the previous one (32, 64) ----
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x & 31;
-        const long long T = (long long)st.ntx * st.nty;
-        const long long s0 = c->s0, s_end = c->s_end;  // written by the prologue kernel
-        const bool loop_mode = c->mode == MODE_LOOP;
-        const double t_next = c->t_next;
-        unsigned long long k = 0;
-        if (lane == 0) {
-            if constexpr (STATIC) {
-                k = sl.next;
-                sl.next = k + gridDim.x;
-            } else {
-                k = atomicAdd(&c->queue, 1ull);
+        // stage block b (step s0 + b/2, stage 1 + b%2), position r; each block visits the tiles in
+        // row-major order starting one tile row further than the block before it (tile r + bm*ntx mod
+        // T), so that a block's first rows depend only on the first rows of the block before it
+        // (never on its last rows through a periodic wrap)
+        long long b;
+        int r, bm;
+        if constexpr (STATIC) {
+            b = sl.b;
+            r = sl.r;
+            bm = sl.bm;
+            __syncwarp();
+            if (lane == 0) {  // advance the CTA's sequence by G items
+                int r2 = r + sl.g_rest, inc = sl.g_blocks;
+                if (r2 >= sl.T) { r2 -= sl.T; ++inc; }
+                sl.b = b + inc;
+                sl.r = r2;
+                sl.bm = int((unsigned)(bm + inc) % (unsigned)st.nty);
             }
+        } else {
+            unsigned long long k = 0;
+            if (lane == 0) k = atomicAdd(&c->queue, 1ull);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            const unsigned long long T = (unsigned long long)sl.T;
+            b = (long long)(k / T);
+            r = int(k - (unsigned long long)b * T);
+            bm = int(b % st.nty);
         }
-        k = __shfl_sync(0xffffffffu, k, 0);
-        // stage block b = k / T (step s0 + b/2, stage 1 + b%2); each block visits the tiles in row-major
-        // order starting one tile row further than the block before it, so that a block's first rows
-        // depend only on the first rows of the block before it (never on its last rows through a
-        // periodic wrap)
-        const long long b = (long long)(k / (unsigned long long)T);
-        const long long step = s0 + b / 2;
+        const long long step = sl.s0 + b / 2;
         const int stage = int(b & 1) + 1;
-        const int tile = int(((long long)(k % (unsigned long long)T) + (b % st.nty) * st.ntx) % T);
-        int go = step < s_end;
+        int tile = r + bm * st.ntx;
+        if (tile >= sl.T) tile -= sl.T;
+        int go = step < sl.s_end;
         double dt = 0.0;
         if (go && stage == 1) {
-            if (step > s0) {
+            if (step > sl.s0) {
                 // step - 1 must run (else nothing will publish its flags) and, in the loop, step
                 // must not start at or past t_next; both are known once step - 2 is published
                 int ok = 1;
                 if (lane == 0) {
-                    ok = wait_complete(c, step - 2) && __ldcg(&c->srun[(step - 1) & 1]) &&
-                         (!loop_mode || __ldcg(&c->t[step & 1]) < t_next);
+                    const int q = published(c, sl, step - 2);
+                    ok = q >= 0 && sl.pub_run[q] && (!sl.loop || sl.pub_t2[q] < sl.t_next);
                 }
                 go = __shfl_sync(0xffffffffu, ok, 0);
                 if (go) go = wait_flags(c, st.flag2, st, tile, unsigned(step));
             } else {
-                go = __ldcg(&c->srun[s0 & 1]);
+                go = __ldcg(&c->srun[sl.s0 & 1]);
             }
         } else if (go) {
             int ok = 1;
             if (lane == 0) {
-                ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
-                dt = __ldcg(&c->sdt[step & 1]);
+                const int q = published(c, sl, step - 1);
+                ok = q >= 0 && sl.pub_run[q];
+                dt = q >= 0 ? sl.pub_dt[q] : 0.0;
             }
             go = __shfl_sync(0xffffffffu, ok, 0);
             if (go) go = wait_flags(c, st.flag1, st, tile, unsigned(step + 1));
@@ -316,11 +383,13 @@ __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* 
             sl.tile = tile;
             sl.dt = dt;
         }
-    } else if (threadIdx.x == kTailThread && sl.prev_stage != 0) {
-        item_tail(g, st, sl);
+    } else if (threadIdx.x == kFlagThread) {
+        if (sl.prev_stage != 0) release_flag(st, sl);
+    } else if (threadIdx.x == kCountThread) {
+        if (sl.prev_stage == 2) count_stage2(g, sl);
     }
     __syncthreads();
-    if (threadIdx.x == kTailThread) {  // the item to complete next time, if it runs to its end
+    if (threadIdx.x == kFlagThread) {  // the item to complete next time, if it runs to its end
         sl.prev_step = sl.step;
         sl.prev_stage = sl.go ? sl.stage : 0;
         sl.prev_tile = sl.tile;
@@ -336,10 +405,9 @@ __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* 
         // stage 1 waits for its step's publication only before its update
         auto pre4 = [&]() -> bool {
             if (threadIdx.x == 0) {
-                const long long step = sl.step;
-                const bool ok = wait_complete(c, step - 1) && __ldcg(&c->srun[step & 1]);
-                sl.dt = __ldcg(&c->sdt[step & 1]);
-                sl.go = ok;
+                const int q = published(c, sl, sl.step - 1);
+                sl.go = q >= 0 && sl.pub_run[q];
+                sl.dt = q >= 0 ? sl.pub_dt[q] : 0.0;
             }
             __syncthreads();
             return sl.go != 0;
@@ -351,11 +419,11 @@ __device__ __forceinline__ bool stepper_item(const GridDesc& g, const TileMaps* 
                                                                                 one, ctl, s, sx, sy, bad);
     }
     if (!done) {  // the step does not run (a bad cell or a timeout stopped the grid): nothing to complete
-        if (threadIdx.x == kTailThread) sl.prev_stage = 0;
+        if (threadIdx.x == kFlagThread) sl.prev_stage = 0;
         return false;
     }
     if (sl.stage == 2) block_wave_speeds<NT>(sx, sy, bad, sl);  // ends with no barrier
-    __syncthreads();  // every store of this item precedes its completion (the next call's item_tail)
+    __syncthreads();  // every store of this item precedes its completion (the next call's)
     return true;
 }
 
@@ -371,9 +439,9 @@ __global__ void __launch_bounds__(NT, MINB) stepper_kernel(const GridDesc g, con
             tc::mbar_init(&s.bar, 1);
             tc::fence_mbar_init();
         }
-        sl.next = blockIdx.x;
+        slot_begin(sl, g, st, true);
     }
-    if (threadIdx.x == kTailThread) sl.prev_stage = 0;
+    __syncthreads();
     uint32_t phase = 0;
     while (stepper_item<FLUX, LIM, TX, TY, NT, true>(g, &tm, st, s, phase, sl)) {
     }
@@ -397,7 +465,6 @@ __global__ void __launch_bounds__(NT, MINB) multi_stepper_kernel(const GridDesc*
     __shared__ GridDesc s_g;      // the current member's descriptors, read from shared memory as needed
     __shared__ StepperTiles s_st;
     __shared__ StepperSlot sl;
-    if (threadIdx.x == kTailThread) sl.prev_stage = 0;
     if (threadIdx.x == 0) {
         if (maps) {
             tc::mbar_init(&s.bar, 1);
@@ -407,6 +474,7 @@ __global__ void __launch_bounds__(NT, MINB) multi_stepper_kernel(const GridDesc*
         if (s_member >= 0) {
             s_g = members[s_member];
             s_st = tiles[s_member];
+            slot_begin(sl, s_g, s_st, false);
         }
     }
     __syncthreads();
@@ -428,6 +496,7 @@ __global__ void __launch_bounds__(NT, MINB) multi_stepper_kernel(const GridDesc*
                 if (next >= 0) {
                     s_g = members[next];
                     s_st = tiles[next];
+                    slot_begin(sl, members[next], tiles[next], false);
                 }
             }
             __syncthreads();
