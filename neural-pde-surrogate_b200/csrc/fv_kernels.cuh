@@ -265,6 +265,9 @@ __device__ __forceinline__ bool tile_body(const GridDesc& g, const TileMaps* tm,
                      (tc::smem_addr(&s.W[0][0][0]) & 127u) == 0;  // the copy's destination alignment
     if (tma) {
         if (threadIdx.x == 0) {
+            // the CTA's generic accesses to s.W before this point (a previous tile of a persistent
+            // CTA, past a CTA barrier) are ordered before the asynchronous proxy's writes
+            tc::fence_proxy_async_smem();
             tc::mbar_arrive_expect_tx(&s.bar, (uint32_t)sizeof(s.W));
             tc::tma_load_4d(&s.W[0][0][0], (STAGE == 1) ? (const void*)&tm->w : (const void*)&tm->w1, 0, i0 - 2,
                             j0 - 2, 0, &s.bar);
