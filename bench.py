@@ -63,14 +63,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+PROFILE_SUMMARIES = ("fv_stepper_kernel_blast512.md", "fv_stage_kernels_blast512.md")
+
+
 def profiled(key):
-    """A figure of the committed ncu summary of the stage kernels ("key: value" line), or None."""
-    f = ROOT / "profiles" / "fv_stage_kernels_blast512.md"
-    if not f.exists():
-        return None
-    for line in f.read_text().splitlines():
-        if line.startswith(key + ":"):
-            return float(line.split(":")[1])
+    """A figure of the committed ncu summaries of the stepper and stage kernels ("key: value" line),
+    or None."""
+    for name in PROFILE_SUMMARIES:
+        f = ROOT / "profiles" / name
+        if not f.exists():
+            continue
+        for line in f.read_text().splitlines():
+            if line.startswith(key + ":"):
+                return float(line.split(":")[1])
     return None
 
 

@@ -49,6 +49,13 @@ def test_roofline_figures_come_from_the_committed_summary():
     assert bench.profiled_traffic() == pytest.approx(bench.STAGE_BYTES[2] * 512 * 512, rel=0.01)
     assert 0.0 < bench.profiled("fp64_pipe_active_stage2") < 1.0
     assert bench.profiled("no_such_figure") is None
+    # the stepper's figures: DRAM bytes per step (L2-resident grid: far below the 160 B/cell of HBM
+    # traffic), executed FP64 flops per cell-step and FP64 pipe activity
+    assert 0 < bench.profiled("traffic_bytes_per_step_stepper") < 160 * 512 * 512
+    assert 500 < bench.profiled("fp64_flops_per_cell_step") < 3000
+    assert 0.0 < bench.profiled("fp64_pipe_active_stepper") < 1.0
+    r = bench.fp64_roofline(512, 0.0415, per="step")  # a 41.5 us step at 512^2
+    assert r["achieved"] == pytest.approx(bench.profiled("fp64_flops_per_cell_step") * 512 * 512 / 41.5e-6 / 1e12)
 
 
 def test_peak_denominator_measured_or_fallback(tmp_path, monkeypatch):
