@@ -461,7 +461,9 @@ def hybrid_leg(n_riemann=6, n_blast=6, n_kh=4, batch=128, frames=100, truth_n=10
                       f"batch of {len(items) + len(extra)} advanced together (those and {len(extra)} more "
                       f"Riemann/blast, indices 300000+)",
             "truth": f"{truth_n}^2 FP64 plain solve, HLLC + van Leer ({truth_s:.0f} s, outside every timed figure)",
-            "hybrid": {"method": f"{coarse}^2 + correction_64.npz, scale mode, gain {gain}",
+            "hybrid": {"method": f"{coarse}^2 + correction_64.npz, scale mode (signal speed at most "
+                                 f"{importlib.import_module(f'{PKG}.correction').MAX_SPEED_RATIO:g}x the coarse "
+                                 f"state's), gain {gain}",
                        **{k: hyb[k] for k in keep}, "fallback_steps": hyb["fallback_steps"],
                        "coarse_retries": hyb["coarse_retries"], "failed": hyb["failed"]},
             "plain": {str(r["n"]): {k: r[k] for k in keep} for r in plains},

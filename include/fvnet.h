@@ -70,14 +70,18 @@ int fvnet_prep_input(const double* U, long long npix, const double* stats, void*
  *                      sees an unphysical correction instead of ignoring it); fallback flags it;
  *   FVNET_CORR_SCALE:  Unext = Uc + theta D with the largest theta in [0,1] keeping every cell's rho
  *                      and p above a tenth of their coarse values (theta = 0 is the plain coarse step);
- *                      theta is uniform over the sample, so theta D is still zero-mean.
+ *                      theta is uniform over the sample, so theta D is still zero-mean.  With
+ *                      max_speed_ratio > 0 theta is then halved (up to 6 times, else 0) until the
+ *                      sample's signal speed max(|u| + a) + max(|v| + a) is at most max_speed_ratio
+ *                      times that of Uc: the next coarse step's CFL dt shrinks at most by that factor.
+ * max_speed_ratio: <= 0 (no bound) or >= 1; used by FVNET_CORR_SCALE only.
  * fallback[b] = 1 when sample b did not receive its full correction; theta (may be NULL) receives
  * the fraction applied. */
 #define FVNET_CORR_STRICT 0
 #define FVNET_CORR_KEEP 1
 #define FVNET_CORR_SCALE 2
 int fvnet_apply_correction(const double* Uc, const float* out4, int B, int npix, const double* dscale, double* Unext,
-                           int* fallback, double* theta, int mode, void* stream);
+                           int* fallback, double* theta, int mode, double max_speed_ratio, void* stream);
 
 /* Loss and gradient: loss_part[b] = sum over the sample of ((Unext - Y) / std)^2 (the loss is the
  * sum of loss_part over b divided by B*npix*4); dout16 [B][npix][16] BF16 = d loss / d out4 through

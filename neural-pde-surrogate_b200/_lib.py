@@ -83,7 +83,7 @@ _PROTOS = {
     "fvnet_wgrad_parts": [_I, _I],
     "fvnet_pack_weights": [_I, _I, _I, _I, _P, _P, _P, _P],
     "fvnet_prep_input": [_P, C.c_longlong, _P, _P, _P],
-    "fvnet_apply_correction": [_P, _P, _I, _I, _P, _P, _P, _P, _I, _P],
+    "fvnet_apply_correction": [_P, _P, _I, _I, _P, _P, _P, _P, _I, _D, _P],
     "fvnet_loss_grad": [_P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P],
     "fvnet_adamw": [_P, _P, _P, _P, C.c_longlong, _P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                     C.c_float, _I, _P, _P],

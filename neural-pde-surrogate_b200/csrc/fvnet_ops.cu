@@ -63,6 +63,8 @@ __device__ __forceinline__ double block_min(double v, double* sh) {
     return r;
 }
 
+__device__ __forceinline__ double block_max(double v, double* sh) { return -block_min(-v, sh); }
+
 // The network predicts corrections relative to the coarse cell: the density and momentum corrections
 // in units of the cell's density, the energy correction in units of its energy (the reference's
 // Positive wrapper, models.py:254-306, works in log-primitive variables for the same reason: an
@@ -102,16 +104,44 @@ __device__ __forceinline__ double admissible_theta(const double* u, const double
     return fmax(0.0, fmin(th, root));
 }
 
+// Signal speed of a sample's state Uc + theta D, as the CFL step sees it on square cells:
+// max(|u| + a) + max(|v| + a) over the cells (solver2d.hpp:67-83 with dx = dy), a = sqrt(gamma p / rho);
+// infinite if a cell is not physical.  Every thread of the CTA calls it and gets the result.
+__device__ __forceinline__ double signal_speed(const double* uc, const float* o, const double* dscale,
+                                               const double* mean, double theta, int npix, double* sh) {
+    double sx = 0.0, sy = 0.0;
+    for (int p = threadIdx.x; p < npix; p += RT) {
+        fv::Q4 u{uc[p * 4 + 0] + theta * (raw_correction(o, uc, dscale, p, 0) - mean[0]),
+                 uc[p * 4 + 1] + theta * (raw_correction(o, uc, dscale, p, 1) - mean[1]),
+                 uc[p * 4 + 2] + theta * (raw_correction(o, uc, dscale, p, 2) - mean[2]),
+                 uc[p * 4 + 3] + theta * (raw_correction(o, uc, dscale, p, 3) - mean[3])};
+        const fv::Q4 w = fv::to_primitive(u);
+        if (!(w.a > 0.0) || !(w.d > 0.0)) {
+            sx = INFINITY;
+            continue;
+        }
+        const double a = sqrt(fv::GAMMA * w.d / w.a);
+        sx = fmax(sx, fabs(w.b) + a);
+        sy = fmax(sy, fabs(w.c) + a);
+    }
+    sx = block_max(sx, sh);
+    sy = block_max(sy, sh);
+    return sx + sy;
+}
+
 // One CTA per sample.  D = out4 * dscale (FP64), D -= mean(D) per field (zero-mean projection), then
 //   mode STRICT: Unext = Uc + D, or Uc if any cell of it has !(rho > 0) || !(p > 0)  (theta 1 or 0)
 //   mode KEEP:   Unext = Uc + D always; theta = 1, fallback flags the non-physical samples
 //   mode SCALE:  Unext = Uc + theta D with the largest theta in [0,1] keeping every cell's rho and p
-//                above a tenth of their coarse values (theta = 0 is the plain coarse step)
+//                above a tenth of their coarse values (theta = 0 is the plain coarse step); with
+//                max_speed_ratio > 0, theta is then halved (up to 6 times, else 0) until the signal
+//                speed of Uc + theta D is at most max_speed_ratio times that of Uc
 // fallback[b] = 1 when the sample did not get its full correction (or, in KEEP mode, would not have).
 __global__ void __launch_bounds__(RT) apply_correction_kernel(const double* __restrict__ Uc, const float* __restrict__ out4,
                                                               int npix, const double* __restrict__ dscale,
                                                               double* __restrict__ Unext, int* __restrict__ fallback,
-                                                              double* __restrict__ theta_out, int mode) {
+                                                              double* __restrict__ theta_out, int mode,
+                                                              double max_speed_ratio) {
     __shared__ double sh[RT];
     __shared__ int sbad;
     const int b = blockIdx.x;
@@ -133,6 +163,16 @@ __global__ void __launch_bounds__(RT) apply_correction_kernel(const double* __re
             tmin = fmin(tmin, admissible_theta(uc + (size_t)p * 4, d));
         }
         theta = block_min(tmin, sh);
+        if (max_speed_ratio > 0.0 && theta > 0.0) {
+            // the coarse step's CFL dt must not shrink by more than the ratio: a correction that
+            // raises the signal speed (a near-vacuum cell, a fast spurious jet) would make the next
+            // coarse step take that many more sub-steps
+            const double limit = max_speed_ratio * signal_speed(uc, o, dscale, mean, 0.0, npix, sh);
+            double th = theta;
+            int k = 0;
+            for (; k <= 6 && signal_speed(uc, o, dscale, mean, th, npix, sh) > limit; ++k) th *= 0.5;
+            theta = (k <= 6) ? th : 0.0;
+        }
     }
     if (threadIdx.x == 0) sbad = 0;
     __syncthreads();
@@ -256,12 +296,12 @@ int fvnet_prep_input(const double* U, long long npix, const double* stats, void*
 }
 
 int fvnet_apply_correction(const double* Uc, const float* out4, int B, int npix, const double* dscale, double* Unext,
-                           int* fallback, double* theta, int mode, void* stream) {
+                           int* fallback, double* theta, int mode, double max_speed_ratio, void* stream) {
     if (!Uc || !out4 || !dscale || !Unext || !fallback || B <= 0 || npix <= 0 || mode < FVNET_CORR_STRICT ||
-        mode > FVNET_CORR_SCALE)
+        mode > FVNET_CORR_SCALE || !(max_speed_ratio <= 0.0 || max_speed_ratio >= 1.0))
         return fv_internal_set_error(FVNET_ERR_ARG, "fvnet_apply_correction: bad arguments");
     apply_correction_kernel<<<B, RT, 0, static_cast<cudaStream_t>(stream)>>>(Uc, out4, npix, dscale, Unext, fallback,
-                                                                             theta, mode);
+                                                                             theta, mode, max_speed_ratio);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FVNET_OK : fv_internal_set_error(FVNET_ERR_CUDA, cudaGetErrorString(e));
 }

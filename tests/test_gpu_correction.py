@@ -265,3 +265,42 @@ def test_network_is_translation_equivariant():
         torch.cuda.synchronize()
         net.check_device_error()
         assert torch.equal(rolled, torch.roll(out, shift, dims=(1, 2))), shift
+
+
+def test_scale_mode_bounds_the_signal_speed():
+    """'scale' with a signal-speed bound: a correction that would raise max(|u|+a) + max(|v|+a) above
+    the ratio times the coarse state's is halved until it does not (or dropped), and stays physical,
+    conservative and no larger than the positivity-only fraction."""
+    B, H, W = 3, 4, 64
+    rng = np.random.default_rng(9)
+    net = corr.CorrectionNet(B, H, W, params=rng.normal(0, 0.2, corr.param_count()).astype(np.float32))
+    Uc = _physical(rng, (B, H, W))
+    stats = _stats().cuda()
+    Un = torch.empty_like(Uc).cuda()
+    fb = torch.zeros(B, dtype=torch.int32, device="cuda")
+    big = torch.tensor([1.0, 30.0, 30.0, 1.0], dtype=torch.float64, device="cuda")  # mostly momentum
+
+    def speed(U):
+        r = U[..., 0]
+        u, v = U[..., 1] / r, U[..., 2] / r
+        a = torch.sqrt(1.4 * 0.4 * (U[..., 3] - 0.5 * r * (u * u + v * v)) / r)
+        return (u.abs() + a).amax(dim=(1, 2)) + (v.abs() + a).amax(dim=(1, 2))
+
+    net.correct(Uc.cuda(), stats, big, Un, fb, mode="scale", max_speed_ratio=0.0)  # positivity only
+    torch.cuda.synchronize()
+    th_free = net.theta.cpu().clone()
+    s_free = speed(Un.cpu())
+    for ratio in (1.2, 2.0):
+        net.correct(Uc.cuda(), stats, big, Un, fb, mode="scale", max_speed_ratio=ratio)
+        torch.cuda.synchronize()
+        th = net.theta.cpu()
+        assert (th <= th_free).all()
+        assert (speed(Un.cpu()) <= ratio * speed(Uc) * (1 + 1e-12)).all()
+        for b in range(B):  # the bound acted only where the free fraction broke it
+            if s_free[b] <= ratio * speed(Uc)[b]:
+                assert th[b] == th_free[b]
+            else:
+                assert th[b] < th_free[b]
+    assert bool((s_free > 1.2 * speed(Uc)).any())  # the case exercises the bound
+    with pytest.raises(Exception):
+        net.correct(Uc.cuda(), stats, big, Un, fb, mode="scale", max_speed_ratio=0.5)  # below 1: rejected
