@@ -576,7 +576,8 @@ def run_stage_case(args):
                       "per_stage_cell_updates_per_s": cells / ((ms1 + ms2) / 1e3),
                       "stepper_steps": k2, "stepper_launches": launches, "stepper_us_per_step": ms_step * 1e3,
                       "stepper_cell_updates_per_s": cells / (ms_step / 1e3) if ms_step > 0 else None,
-                      "stepper_tile": solver.stepper_tile(s), "build": os.environ.get("FV_BUILD", "parity")}),
+                      "stepper_tile": solver.stepper_tile(s), "stepper_launch": solver.stepper_launch(s),
+                      "build": os.environ.get("FV_BUILD", "parity")}),
           flush=True)
 
 

@@ -214,6 +214,10 @@ int fv_profile_steps(fv_solver* s, double* ms_per_step, long long* steps, long l
  * stepper is switched off).  Chosen like the per-stage kernels' shape, by timing each on a copy of
  * the state; FV_STEPPER_TILE=<index> fixes it. */
 int fv_stepper_tile(fv_solver* s, int* tx, int* ty, int* threads);
+/* The stepper shape's index (what FV_STEPPER_TILE takes) and its launch: CTAs per SM and CTAs in
+ * all; -1 and 0s before the first fv_advance_to or with the stepper switched off.  Any pointer may
+ * be NULL. */
+int fv_stepper_launch(fv_solver* s, int* variant, int* ctas_per_sm, int* ctas);
 
 /* Self-test of the library's bounded waits: runs the wait used for every TMA copy and tensor-core
  * batch on a barrier that nothing arrives at, with a 10 ms limit.  Returns FV_ERR_TIMEOUT when the

@@ -62,6 +62,7 @@ _PROTOS = {
     "fv_profile_read": [_P, _DP, _DP, _LLP],
     "fv_profile_steps": [_P, _DP, _LLP, _LLP],
     "fv_stepper_tile": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
+    "fv_stepper_launch": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
     "fv_stepper_dependencies": [_I, _I, _I, _I, _I, _I, _P, _I, _P, _I, C.POINTER(_I)],
     "fv_launch_count": [_P, _LLP],
     "fv_fp64_peak": [_DP],

@@ -119,6 +119,7 @@ const std::vector<StepperVariant>& stepper_variants() {
         StepperMaker<16, 7, 128, 8>::make(8),   // 3
         StepperMaker<32, 16, 512, 2>::make(1),  // 4
         StepperMaker<16, 7, 128, 9>::make(10),  // 5: 36 warps per SM at <= 56 registers
+        StepperMaker<32, 14, 512, 2>::make(7),  // 6: 512^2 -> 592 tiles, exactly 2 per CTA and stage
     };
     return v;
 }
@@ -1117,6 +1118,17 @@ int fv_profile_steps(fv_solver* s, double* ms_per_step, long long* steps, long l
     if (ms_per_step) *ms_per_step = n ? ms / n : 0.0;
     if (steps) *steps = n;
     if (launches) *launches = s->step_launches;
+    return FV_OK;
+}
+
+int fv_stepper_launch(fv_solver* s, int* variant, int* ctas_per_sm, int* ctas) {
+    if (!s) return set_error(FV_ERR_ARG, "fv_stepper_launch: NULL handle");
+    const bool on = stepper_enabled() && s->svariant >= 0 && s->sgrid > 0;
+    int sms = 1;
+    if (on) FV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    if (variant) *variant = on ? s->svariant : -1;
+    if (ctas_per_sm) *ctas_per_sm = on ? s->sgrid / sms : 0;
+    if (ctas) *ctas = on ? s->sgrid : 0;
     return FV_OK;
 }
 

@@ -287,6 +287,14 @@ def stepper_tile(solver):
     return a.value, b.value, c.value
 
 
+def stepper_launch(solver):
+    """(shape index, CTAs per SM, CTAs) of the handle's persistent stepper; (-1, 0, 0) before its
+    first use."""
+    v, per_sm, ctas = C.c_int(), C.c_int(), C.c_int()
+    check(lib().fv_stepper_launch(solver._h, C.byref(v), C.byref(per_sm), C.byref(ctas)))
+    return v.value, per_sm.value, ctas.value
+
+
 def launch_count(solver):
     n = C.c_longlong()
     check(lib().fv_launch_count(solver._h, C.byref(n)))

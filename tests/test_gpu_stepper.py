@@ -51,10 +51,12 @@ np.savez(sys.argv[3], **out)
 """
 
 
-def _run(tmp_path, stepper, **case):
+def _run(tmp_path, stepper, tile=None, **case):
     inp, out = tmp_path / "case.npz", tmp_path / f"out{stepper}.npz"
     np.savez(inp, **case)
     env = dict(os.environ, FV_STEPPER=str(stepper))
+    if tile is not None:
+        env["FV_STEPPER_TILE"] = str(tile)
     r = subprocess.run([sys.executable, "-c", CHILD, str(ROOT), str(inp), str(out)], env=env, capture_output=True,
                        text=True, timeout=900)
     assert r.returncode == 0, r.stderr
@@ -138,3 +140,23 @@ def test_stepper_long_run_spans_several_launches(cuda_ok, tmp_path):
     for k in range(20):
         assert b[f"n{k}"] == o[f"n{k}"] and b[f"t{k}"] == o[f"t{k}"]
     assert bits_equal(b["U"], o["U"])
+
+
+# (tile width, height, threads) of each stepper shape, in the library's order
+STEPPER_SHAPES = [(16, 14, 256), (16, 16, 256), (32, 8, 256), (16, 7, 128), (32, 16, 512), (16, 7, 128),
+                  (32, 14, 512)]
+
+
+@pytest.mark.parametrize("shape", range(len(STEPPER_SHAPES)))
+def test_every_stepper_shape_is_bitexact(cuda_ok, tmp_path, shape):
+    """Each tile shape of the stepper (FV_STEPPER_TILE fixes it instead of the autotuner) on a grid
+    with partial edge tiles in both directions and a transmissive boundary, against the oracle."""
+    nx, ny = 70, 45
+    case = dict(nx=nx, ny=ny, ly=45 / 70, bcx="periodic", bcy="transmissive", flux="hllc", lim="vanleer",
+                U0=_random(nx, ny, 40 + shape), targets=np.array([0.02, 0.03]), mix_step=False)
+    got = _run(tmp_path, 1, tile=shape, **case)
+    assert tuple(int(x) for x in got["tile"]) == STEPPER_SHAPES[shape]
+    ref = _oracle(case)
+    for k in range(2):
+        assert float(got[f"t{k}"]) == ref[f"t{k}"] and int(got[f"n{k}"]) == ref[f"n{k}"]
+    assert bits_equal(got["U"], ref["U"])
