@@ -221,18 +221,19 @@ __global__ void __launch_bounds__(NT) conv3x3_rows_kernel(ConvArgs a) {
         tc::mbar_init(bar, 1);
         tc::fence_mbar_init();
     }
-    // stage rows y0-1 .. y0+TR (periodic in y) once, with the periodic x-neighbours at both ends
-#pragma unroll 4
+    // stage rows y0-1 .. y0+TR (periodic in y) once, with the periodic x-neighbours at both ends, and
+    // the weights: asynchronous 16-byte copies, all in flight together, then one wait
     for (int e = tid; e < (TR + 2) * W * CC; e += NT) {
         const int cc = e % CC, t = e / CC, x = t % W, r = t / W;
         const int y = (y0 - 1 + r + H) % H;
-        const uint4 v = a.X[(size_t(n * H + y) * W + x) * CC + cc];
+        const uint4* src = a.X + (size_t(n * H + y) * W + x) * CC + cc;
         uint4* row = Xs + size_t(cc) * PS + r * W2;
-        row[x + 1] = v;
-        if (x == W - 1) row[0] = v;
-        if (x == 0) row[W + 1] = v;
+        tc::cp_async16(row + x + 1, src);
+        if (x == W - 1) tc::cp_async16(row, src);
+        if (x == 0) tc::cp_async16(row + W + 1, src);
     }
-    for (int e = tid; e < 9 * CC * COUT; e += NT) Wt[e] = a.Wb[e];
+    for (int e = tid; e < 9 * CC * COUT; e += NT) tc::cp_async16(Wt + e, a.Wb + e);
+    tc::cp_async_wait_all();
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();

@@ -71,6 +71,15 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0,
         : "memory");
 }
 
+// ---- per-thread asynchronous copies ------------------------------------------------------------
+// 16 bytes global -> shared without a round trip through registers (both addresses 16-byte aligned);
+// cp_async_wait_all waits for all of this thread's copies.  The data are then visible to the thread
+// itself; a CTA barrier makes them visible to the others.
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src_global) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst_smem)), "l"(src_global) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ---- fences --------------------------------------------------------------------------------------
 // Generic-proxy shared-memory writes made visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
