@@ -45,7 +45,7 @@ def test_reference_arm_runs_on_rank_zero_only():
 
 
 def test_roofline_figures_come_from_the_committed_summary():
-    assert bench.profiled_traffic() == 25204992.0  # DRAM bytes per stage-2 launch at 512^2
+    assert bench.profiled_traffic() == 25213952.0  # DRAM bytes per stage-2 launch at 512^2
     assert bench.profiled_traffic() == pytest.approx(bench.STAGE_BYTES[2] * 512 * 512, rel=0.01)
     assert 0.0 < bench.profiled("fp64_pipe_active_stage2") < 1.0
     assert bench.profiled("no_such_figure") is None
@@ -87,10 +87,10 @@ def test_clock_summary_flags_slowdowns(tmp_path):
 
 def test_fp64_roofline_of_the_stage_kernel(tmp_path, monkeypatch):
     r = bench.fp64_roofline(512, 0.0238)  # a 23.8 us stage-1 launch at 512^2
-    assert r["unit"] == "TFLOP/s" and r["flops_per_cell"] == 542.0 and r["peak"] == 36.2
-    assert r["achieved"] == pytest.approx(542 * 512 * 512 / 23.8e-6 / 1e12)  # ~5.97 TFLOP/s
+    assert r["unit"] == "TFLOP/s" and r["flops_per_cell"] == 548.0 and r["peak"] == 36.2
+    assert r["achieved"] == pytest.approx(548 * 512 * 512 / 23.8e-6 / 1e12)  # ~6.04 TFLOP/s
     assert r["frac"] == pytest.approx(r["achieved"] / 36.2) and 0.1 < r["frac"] < 0.25
-    assert r["pipe_active_ncu"] == 0.407
+    assert r["pipe_active_ncu"] == 0.433
     assert bench.fp64_roofline(512, 0.0) is None  # no timed launches
     monkeypatch.setattr(bench, "ROOT", tmp_path)  # no committed summary: no figure, no error
     assert bench.fp64_roofline(512, 0.0238) is None
