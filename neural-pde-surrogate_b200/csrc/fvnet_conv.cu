@@ -16,9 +16,12 @@
 // TMEM; the epilogue (tcgen05.ld, one accumulator row per thread) adds the bias and applies GELU, or
 // for the backward-data pass multiplies by GELU'(pre-activation of the layer below).
 // Backward data is the same kernel with the weights transposed (c_in <-> c_out) and flipped.
-// Backward weights (M = 9 * c_in, N = c_out, K = pixels): per image row, the shifted input rows and
-// the output gradient are transposed into K-major tiles and accumulated in TMEM over the CTA's rows;
-// per-CTA partial sums are reduced in a fixed order (deterministic).
+// Image widths >= 64 use a row kernel that stages each input row once and takes the x-shifts as
+// descriptor offsets of M = 64 tiles (conv3x3_rows_kernel).
+// Backward weights (per x-shift: M = 3 * c_in rows (ky, c_in), N = c_out, K = pixels): per image row
+// the MMAs read the staged input rows and output-gradient row in place as MN-major operands and
+// accumulate in TMEM over the CTA's rows; per-CTA partial sums are reduced in a fixed order
+// (deterministic).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -320,26 +323,35 @@ struct WgradArgs {
     int* err;
 };
 
-__host__ __device__ constexpr int wgrad_mrows(int cin) { return ((9 * cin + 127) / 128) * 128; }
-// Staged input / output-gradient rows keep 8 extra channels per pixel (16 bytes): the 8 pixel rows an
-// ldmatrix reads are then 80 (or 48) bytes apart instead of 64 (or 32) and fall in distinct bank groups.
-__host__ __device__ constexpr size_t wgrad_smem_bytes(int cin, int cout, int W) {
-    return size_t(W / 8) * wgrad_mrows(cin) * 16 + size_t(W / 8) * cout * 16 + size_t(3) * W * (cin + 8) * 2 +
-           size_t(W) * (cout + 8) * 2 + 64;
+// ---- backward weights, operands read in place (MN-major) ----------------------------------------
+// dW[(ky, kx, ci)][co] = sum over pixels of X[y + ky - 1][x + kx - 1][ci] dZ[y][x][co].  Per output row y
+// and x-shift kx one accumulator D_kx[(ky, ci)][co] (M = 3 CIN rows, padded to 64 or 128; N = COUT; K =
+// the row's pixels), and the MMAs read the staged rows themselves: a chunk of 8 channels is 16
+// contiguous bytes per pixel and consecutive pixels are 16 bytes apart, which is the canonical
+// no-swizzle MN-major layout (instruction descriptor major bits set; LBO = 128 bytes between groups
+// of 8 pixels, SBO = the chunk stride).  There are no operand transposes.
+// Input rows live in a 4-slot ring, each row stored twice (planes s and s + 4, s = (u + 1) mod 4 for
+// image row u), so that the rows y - 1, y, y + 1 and one more are always 4 consecutive planes of CC
+// chunks: the M rows (ky, ci) then have one chunk stride.  The fourth plane only feeds M rows past
+// 3 CIN, whose results are not used; it is the slot the next row's input is prefetched into while the
+// current row's MMAs run.  The output-gradient rows alternate between two buffers.
+__host__ __device__ constexpr size_t wgrad_mn_smem_bytes(int cin, int cout, int W) {
+    // at least 46 KB: at most 4 CTAs per SM, so that their TMEM (up to 128 columns each) always fits
+    const size_t b = size_t(8) * (cin / 8) * (W + 2) * 16 + size_t(2) * (cout / 8) * W * 16 + 64;
+    return b < 46 * 1024 ? 46 * 1024 : b;
 }
 
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
-    constexpr int M9 = 9 * CIN, MROWS = wgrad_mrows(CIN), MT = MROWS / 128, CC = CIN / 8, OC = COUT / 8;
-    constexpr uint32_t kCols = (MT * COUT) <= 32 ? 32 : ((MT * COUT) <= 64 ? 64 : 128);
+__global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
+    constexpr int CC = CIN / 8, OC = COUT / 8, M9 = 9 * CIN;
+    constexpr int MM = (3 * CIN) <= 64 ? 64 : 128;  // MMA M
+    static_assert(3 * CIN <= 128, "three input rows of CIN channels fit one M = 128 accumulator");
+    constexpr uint32_t kCols = (3 * COUT) <= 32 ? 32 : ((3 * COUT) <= 64 ? 64 : 128);
     extern __shared__ __align__(1024) unsigned char smem[];
-    const int W = a.W, H = a.H, KC = W / 8;
-    uint4* As = reinterpret_cast<uint4*>(smem);                 // [KC][MROWS]
-    uint4* Bs = As + size_t(KC) * MROWS;                        // [KC][COUT]
-    constexpr int XP = CIN + 8, DP = COUT + 8;                   // padded pixel strides (bf16 elements)
-    __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(Bs + KC * COUT);  // [3][W][XP]
-    __nv_bfloat16* Ds = Xs + 3 * W * XP;                         // [W][DP]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + W * DP);
+    const int W = a.W, H = a.H, W2 = W + 2;
+    uint4* Xs = reinterpret_cast<uint4*>(smem);    // [8 planes][CC][W + 2]: pixels x = -1 .. W
+    uint4* Ds = Xs + size_t(8) * CC * W2;          // [2][OC][W]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + size_t(2) * OC * W);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int total = a.B * H;
@@ -350,132 +362,89 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_kernel(WgradArgs a) {
         tc::mbar_init(bar, 1);
         tc::fence_mbar_init();
     }
-    for (int e = tid; e < KC * MROWS; e += NT) As[e] = make_uint4(0, 0, 0, 0);  // padding rows stay zero
+    // input row u (image n, u in [-1, H], periodic) into its two planes, with the periodic x-neighbours
+    auto stage_x = [&](int n, int u) {
+        const int yr = (u + H) % H, s = (u + 1) & 3;
+        const uint4* src = a.X + size_t(n * H + yr) * W * CC;
+        for (int e = tid; e < W * CC; e += NT) {
+            const int x = e / CC, cc = e - x * CC;
+            for (int p = s; p < 8; p += 4) {
+                uint4* row = Xs + (size_t(p) * CC + cc) * W2;
+                tc::cp_async16(row + x + 1, src + e);
+                if (x == W - 1) tc::cp_async16(row, src + e);
+                if (x == 0) tc::cp_async16(row + W + 1, src + e);
+            }
+        }
+    };
+    auto stage_dz = [&](int n, int y, int buf) {  // output-gradient row y into buffer buf: [oc][x]
+        const uint4* src = a.dZ + size_t(n * H + y) * W * OC;
+        for (int e = tid; e < W * OC; e += NT) {
+            const int x = e / OC, oc = e - x * OC;
+            tc::cp_async16(Ds + (size_t(buf) * OC + oc) * W + x, src + e);
+        }
+    };
+    int cur = 0;
+    if (r0 < r1) {
+        const int n = r0 / H, y = r0 % H;
+        stage_x(n, y - 1); stage_x(n, y); stage_x(n, y + 1);
+        stage_dz(n, y, 0);
+    }
+    tc::cp_async_wait_all();
+    tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, COUT);
-    const uint32_t ab = tc::smem_addr(As), bb = tc::smem_addr(Bs);
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(MM, COUT) | (1u << 15) | (1u << 16);  // A and B MN-major
+    const uint32_t xb = tc::smem_addr(Xs), db = tc::smem_addr(Ds);
+    const uint32_t sbo_a = uint32_t(W2) * 16, sbo_b = uint32_t(W) * 16;
     uint32_t phase = 0;
     bool ok = true;
-    uint4* Xs4 = reinterpret_cast<uint4*>(Xs);
-    uint4* Ds4 = reinterpret_cast<uint4*>(Ds);
-    // Input rows y-1, y, y+1 live in a 3-slot ring keyed by the unwrapped row index u in [-1, H] (slot
-    // (u + 3) % 3; row u holds image row (u + H) % H).  A row that continues the previous one in the
-    // same image needs one new input row (u = y + 1, into the slot of u = y - 2) and its output-
-    // gradient row: those are prefetched into registers while the previous row is transposed, and
-    // stored once its transposes are done.  Rows that start a range or an image load all three.
-    constexpr int PF = 4;  // prefetch chunks per thread: W * CC / NT and W * OC / NT are at most 4
-    auto stage_rows = [&](int row, bool all) {  // synchronous load of a row's data into the ring
-        const int n = row / H, y = row % H;
-        for (int e = tid; e < (all ? 3 : 1) * W * CC; e += NT) {
-            const int cc = e % CC, t = e / CC, x = t % W;
-            const int ky = all ? t / W : 2;
-            const int u = y + ky - 1, slot = (u + 3) % 3;
-            Xs4[(slot * W + x) * (CC + 1) + cc] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
-        }
-        for (int e = tid; e < W * OC; e += NT) Ds4[(e / OC) * (OC + 1) + e % OC] = a.dZ[size_t(n * H + y) * W * OC + e];
-    };
-    if (r0 < r1) stage_rows(r0, true);
-    __syncthreads();
     for (int row = r0; row < r1 && ok; ++row) {
         const int n = row / H, y = row % H;
-        const int nrow = row + 1;
-        const bool has_next = nrow < r1, next_cont = has_next && (nrow % H) != 0;
-        uint4 xpre[PF], dpre[PF];
-        if (next_cont) {  // issue the next row's loads now; they land during the transposes
-            const int yn = nrow % H, u = yn + 1;
-#pragma unroll
-            for (int k = 0; k < PF; ++k) {
-                const int e = tid + k * NT;
-                if (e < W * CC) {
-                    const int cc = e % CC, x = e / CC;
-                    xpre[k] = a.X[(size_t(n * H + (u + H) % H) * W + x) * CC + cc];
-                }
-                if (e < W * OC) dpre[k] = a.dZ[size_t(n * H + yn) * W * OC + e];
-            }
-        }
-        // A[kc][m = shift*CIN + ci] = X[y+ky-1][kc*8 + i + kx - 1][ci], i = 0..7 (periodic), and
-        // B[kc][co] = dZ[kc*8 + i][co]: 8x8 bf16 transposes, four per warp instruction pair.  Lane l
-        // names row l%8 of matrix l/8: ldmatrix.trans reads 8 pixel rows (16 bytes = 8 channels each)
-        // and stmatrix writes them back as 8 channel rows of 8 pixels -- one K-major core-matrix row
-        // each.
-        {
-            const int r8 = lane & 7, mq = lane >> 3;
-            constexpr int NA = 9 * CC;  // matrices per kc for A
-            constexpr int NW = NT / 32, ILP = 4;
-            const int na = KC * NA, nops = (na + KC * OC) / 4;  // x4 operations (4 matrices each)
-            const uint32_t xsb = tc::smem_addr(Xs), dsb = tc::smem_addr(Ds);
-            // warp w takes operations w, w + NW, ...; ILP of them at a time: all loads, then all stores
-            for (int k0 = warp; k0 < nops; k0 += ILP * NW) {
-                uint32_t v[ILP][4], dst[ILP];
-#pragma unroll
-                for (int j = 0; j < ILP; ++j) {
-                    const int k = k0 + j * NW;  // warp-uniform
-                    if (k >= nops) break;
-                    const int q = 4 * k + mq;
-                    uint32_t src;
-                    if (q < na) {
-                        const int kc = q / NA, rest = q - kc * NA, sh = rest / CC, cc = rest - sh * CC;
-                        const int ky = sh / 3, kx = sh - ky * 3, slot = (y + ky - 1 + 3) % 3;
-                        int xs = kc * 8 + r8 + kx - 1;
-                        xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
-                        src = xsb + uint32_t(((slot * W + xs) * XP + cc * 8) * 2);
-                        dst[j] = ab + uint32_t((kc * MROWS + sh * CIN + cc * 8 + r8) * 16);
-                    } else {
-                        const int qb = q - na, kc = qb / OC, oc = qb - kc * OC;
-                        src = dsb + uint32_t(((kc * 8 + r8) * DP + oc * 8) * 2);
-                        dst[j] = bb + uint32_t((kc * COUT + oc * 8 + r8) * 16);
-                    }
-                    tc::ldsm_x4_trans(src, v[j][0], v[j][1], v[j][2], v[j][3]);
-                }
-#pragma unroll
-                for (int j = 0; j < ILP; ++j) {
-                    if (k0 + j * NW >= nops) break;
-                    tc::stsm_x4(dst[j], v[j][0], v[j][1], v[j][2], v[j][3]);
-                }
-            }
-        }
-        tc::fence_proxy_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();  // transposes done: A/B complete, and the ring slot of u = y - 1 is free
-        tc::fence_after_sync();
         if (tid == 0) {
-            for (int mt = 0; mt < MT; ++mt)
-                for (int ks = 0; ks < KC / 2; ++ks) {
-                    const uint32_t aa = ab + (2 * ks * MROWS + mt * 128) * 16;
-                    const uint32_t ba = bb + (2 * ks * COUT) * 16;
-                    tc::mma_bf16(tmem + mt * COUT, tc::smem_desc(aa, MROWS * 16, 128), tc::smem_desc(ba, COUT * 16, 128),
-                                 idesc, (row > r0 || ks > 0) ? 1u : 0u);
+            const int p0 = y & 3;  // planes p0 .. p0 + 2 hold rows y - 1, y, y + 1
+            for (int kx = 0; kx < 3; ++kx)
+                for (int ks = 0; ks < W / 16; ++ks) {
+                    const uint32_t aa = xb + (uint32_t(p0 * CC) * W2 + 16 * ks + kx) * 16;
+                    const uint32_t ba = db + (uint32_t(cur * OC) * W + 16 * ks) * 16;
+                    tc::mma_bf16(tmem + kx * COUT, tc::smem_desc(aa, 128, sbo_a), tc::smem_desc(ba, 128, sbo_b), idesc,
+                                 (row > r0 || ks > 0) ? 1u : 0u);
                 }
             tc::mma_commit(bar);
         }
-        // the next row's data into the ring (the MMAs read only A and B)
-        if (next_cont) {
-            const int slot = (nrow % H + 1 + 3) % 3;
-#pragma unroll
-            for (int k = 0; k < PF; ++k) {
-                const int e = tid + k * NT;
-                if (e < W * CC) Xs4[(slot * W + e / CC) * (CC + 1) + e % CC] = xpre[k];
-                if (e < W * OC) Ds4[(e / OC) * (OC + 1) + e % OC] = dpre[k];
-            }
-        } else if (has_next) {
-            stage_rows(nrow, true);
+        const int nrow = row + 1;
+        const bool has_next = nrow < r1, next_cont = has_next && (nrow % H) != 0;
+        if (next_cont) {  // during the MMAs: input row y + 2 (the slot of the unused fourth plane), dZ row y + 1
+            stage_x(n, y + 2);
+            stage_dz(n, y + 1, cur ^ 1);
         }
-        ok = tc::mbar_wait_bounded(bar, phase, a.err);  // A and B are rewritten by the next row
+        ok = tc::mbar_wait_bounded(bar, phase, a.err);
         phase ^= 1;
         tc::fence_after_sync();
+        if (has_next && !next_cont) {  // a new image: its three rows, now that the MMAs are done
+            const int n2 = nrow / H;
+            stage_x(n2, -1); stage_x(n2, 0); stage_x(n2, 1);
+            stage_dz(n2, 0, cur ^ 1);
+        }
+        tc::cp_async_wait_all();
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
         __syncthreads();  // the next row's data is visible
+        tc::fence_after_sync();
+        cur ^= 1;
     }
     if (ok && r0 < r1) {
-        for (int mt = 0; mt < MT; ++mt) {
+        for (int kx = 0; kx < 3; ++kx) {
             float acc[32];
-            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + mt * COUT;
+            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + kx * COUT;
             if constexpr (COUT == 32) tc::tmem_ld_32x32(taddr, acc);
             else tc::tmem_ld_32x16(taddr, acc);
-            const int m = mt * 128 + warp * 32 + lane;
-            if (m < M9) {
+            // M = 128: accumulator row m in lane m; M = 64: rows 16q .. 16q+15 in lanes 32q .. 32q+15
+            const int mrow = (MM == 128) ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : 3 * CIN);
+            if (mrow < 3 * CIN) {
+                const int ky = mrow / CIN, ci = mrow - ky * CIN;
+                const int m = (ky * 3 + kx) * CIN + ci;
                 float* dst = a.partial + (size_t(blockIdx.x) * M9 + m) * COUT;
 #pragma unroll
                 for (int c = 0; c < COUT; ++c) dst[c] = acc[c];
@@ -586,15 +555,14 @@ int launch_conv(const ConvArgs& a, cudaStream_t st) {
 
 template <int CIN, int COUT>
 int launch_wgrad(const WgradArgs& a, int nparts, cudaStream_t st) {
-    const size_t smem = wgrad_smem_bytes(CIN, COUT, a.W);
     static bool attr = false;
     if (!attr) {  // the limit for the largest image width served (W = 128)
-        if (cudaFuncSetAttribute(conv3x3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)wgrad_smem_bytes(CIN, COUT, 128)) != cudaSuccess)
+        if (cudaFuncSetAttribute(conv3x3_wgrad_mn_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)wgrad_mn_smem_bytes(CIN, COUT, 128)) != cudaSuccess)
             return fv_internal_set_error(FVNET_ERR_CUDA, "fvnet: smem attribute");
         attr = true;
     }
-    conv3x3_wgrad_kernel<CIN, COUT><<<nparts, NT, smem, st>>>(a);
+    conv3x3_wgrad_mn_kernel<CIN, COUT><<<nparts, NT, wgrad_mn_smem_bytes(CIN, COUT, a.W), st>>>(a);
     return FVNET_OK;
 }
 
