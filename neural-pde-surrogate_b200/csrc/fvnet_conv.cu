@@ -456,17 +456,18 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
     if (warp == 0) tc::tmem_dealloc(tmem, kCols);
 }
 
-// dW[co][ci][ky][kx] = sum over CTAs (fixed order) of partial[cta][(ky*3+kx)*cin_pad + ci][co]
+// dW[co][ci][ky][kx] = sum over CTAs (fixed order) of partial[cta][(ky*3+kx)*cin_pad + ci][co].  Thread
+// f = (k*cin + ci)*cout + co: consecutive threads read consecutive co of a partial (coalesced).
 __global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int nparts, int cin_pad, int cout_pad,
                                     int cin, int cout, float* __restrict__ dW) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= cout * cin * 9) return;
-    const int k = e % 9, ci = (e / 9) % cin, co = e / (9 * cin);
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= cout * cin * 9) return;
+    const int co = f % cout, ci = (f / cout) % cin, k = f / (cout * cin);
     const size_t stride = size_t(9) * cin_pad * cout_pad;
     const size_t off = (size_t(k) * cin_pad + ci) * cout_pad + co;
     float s = 0.0f;
     for (int p = 0; p < nparts; ++p) s += partial[p * stride + off];
-    dW[e] = s;
+    dW[(size_t(co) * cin + ci) * 9 + k] = s;
 }
 
 // db[co] = sum over pixels of dZ[p][co]: block partials, then a fixed-order sum.  A thread reads whole
@@ -614,7 +615,9 @@ int fvnet_conv3x3(int mode, int cin_pad, int cout_pad, int B, int H, int W, cons
     return FVNET_OK;
 }
 
-int fvnet_wgrad_parts(int B, int H) { return std::max(1, std::min(2 * 148, B * H)); }  // 2 CTAs per SM at W <= 64
+// 2 CTAs per SM (296 partial sums): 3 or 4 per SM were slower (more partial sums to reduce), 1 per SM
+// within 1 %
+int fvnet_wgrad_parts(int B, int H) { return std::max(1, std::min(2 * 148, B * H)); }
 
 int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int H, int W, const void* X, const void* dZ,
                         float* partial, float* dW, float* db, float* db_part, int* err, void* stream) {
