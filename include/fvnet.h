@@ -44,8 +44,9 @@ int fvnet_conv3x3(int mode, int cin_pad, int cout_pad, int B, int H, int W, cons
 
 /* Weight and bias gradients of a layer (cin -> cout, padded cin_pad -> cout_pad) from its input X
  * [B][H][W][cin_pad] and output gradient dZ [B][H][W][cout_pad], both BF16, on the tensor cores
- * (M = 9*cin, N = cout, K = pixels).  dW: [cout][cin][3][3] FP32, db: [cout] FP32.  Workspace:
- * partial >= fvnet_wgrad_parts(B, H) * 9 * cin_pad * cout_pad floats, db_part >= 64 * cout floats.
+ * (per x-shift: M = 3*cin rows (ky, ci), N = cout, K = pixels).  dW: [cout][cin][3][3] FP32, db: [cout]
+ * FP32.  Workspace: partial >= fvnet_wgrad_parts(B, H) * 9 * cin_pad * cout_pad floats,
+ * db_part >= fvnet_wgrad_parts(B, H) * cout_pad floats.
  * W in {32, 64, 128}. */
 int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int H, int W, const void* X, const void* dZ,
                         float* partial, float* dW, float* db, float* db_part, int* err, void* stream);

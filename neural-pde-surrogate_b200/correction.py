@@ -110,7 +110,7 @@ class CorrectionNet:
         self.dZ = [torch.empty((B, H, W, 32), dtype=bf16, device=device) for _ in range(2)]
         parts = lib().fvnet_wgrad_parts(B, H)
         self.partial = torch.empty(parts * 9 * 32 * 32, dtype=torch.float32, device=device)
-        self.db_part = torch.empty(64 * 32, dtype=torch.float32, device=device)
+        self.db_part = torch.empty(parts * 32, dtype=torch.float32, device=device)
         self.norm_part = torch.empty(lib().fvnet_norm_partials(), dtype=torch.float64, device=device)
         self.norm = torch.zeros(1, dtype=torch.float64, device=device)
         self.err = torch.zeros(1, dtype=torch.int32, device=device)

@@ -318,6 +318,7 @@ struct WgradArgs {
     const uint4* X;   // [B][H][W][CIN]
     const uint4* dZ;  // [B][H][W][COUT]
     float* partial;   // [gridDim.x][9*CIN][COUT]
+    float* db_part;   // [gridDim.x][COUT]: the bias gradient of each CTA's rows
     int B, H, W;
     int rows_per_cta;
     int* err;
@@ -400,6 +401,7 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
     const uint32_t sbo_a = uint32_t(W2) * 16, sbo_b = uint32_t(W) * 16;
     uint32_t phase = 0;
     bool ok = true;
+    float bacc = 0.0f;
     for (int row = r0; row < r1 && ok; ++row) {
         const int n = row / H, y = row % H;
         if (tid == 0) {
@@ -418,6 +420,11 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
         if (next_cont) {  // during the MMAs: input row y + 2 (the slot of the unused fourth plane), dZ row y + 1
             stage_x(n, y + 2);
             stage_dz(n, y + 1, cur ^ 1);
+        }
+        {  // the bias gradient: thread t sums channel t % COUT over pixels t / COUT, + NT / COUT, .. of the row
+            const __nv_bfloat16* dz = reinterpret_cast<const __nv_bfloat16*>(Ds + size_t(cur) * OC * W);
+            const int co = tid % COUT;
+            for (int x = tid / COUT; x < W; x += NT / COUT) bacc += __bfloat162float(dz[(size_t(co / 8) * W + x) * 8 + co % 8]);
         }
         ok = tc::mbar_wait_bounded(bar, phase, a.err);
         phase ^= 1;
@@ -451,8 +458,15 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
             }
         }
     }
+    __shared__ float sb[NT];
+    sb[tid] = bacc;
     tc::fence_before_sync();
     __syncthreads();
+    if (ok && r0 < r1 && tid < COUT) {  // the CTA's bias gradient, its threads' sums in a fixed order
+        float b = 0.0f;
+        for (int k = tid; k < NT; k += COUT) b += sb[k];
+        a.db_part[size_t(blockIdx.x) * COUT + tid] = b;
+    }
     if (warp == 0) tc::tmem_dealloc(tmem, kCols);
 }
 
@@ -470,35 +484,14 @@ __global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int npart
     dW[(size_t(co) * cin + ci) * 9 + k] = s;
 }
 
-// db[co] = sum over pixels of dZ[p][co]: block partials, then a fixed-order sum.  A thread reads whole
-// 16-byte chunks (8 channels of one pixel), consecutive threads consecutive chunks (coalesced), and
-// keeps 8 channel sums; the block then sums each channel over its threads in a fixed order.
-__global__ void __launch_bounds__(NT) bias_grad_partial_kernel(const uint4* __restrict__ dZ, long long npix, int cq,
-                                                               int cout, float* __restrict__ part) {
-    __shared__ float s[NT][9];  // padded: the column reads below hit distinct banks
-    const int t = threadIdx.x, q = t % cq, lp = t / cq, ppb = NT / cq;  // cq = cout_pad / 8 chunks per pixel
-    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    for (long long p = (long long)blockIdx.x * ppb + lp; p < npix; p += (long long)gridDim.x * ppb) {
-        const uint4 u = dZ[p * cq + q];
-        const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&u);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] += __bfloat162float(b[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) s[t][j] = acc[j];
-    __syncthreads();
-    if (t < cq * 8) {
-        const int qq = t / 8, j = t % 8, c = 8 * qq + j;
-        float sum = 0.0f;
-        for (int k = qq; k < NT; k += cq) sum += s[k][j];
-        if (c < cout) part[blockIdx.x * cout + c] = sum;
-    }
-}
-__global__ void bias_grad_reduce_kernel(const float* __restrict__ part, int nparts, int cout, float* __restrict__ db) {
+// db[co] = sum over pixels of dZ[p][co]: the weight-gradient kernel leaves each CTA's sum over its rows
+// in db_part[cta][co] (cout_pad per CTA); this sums them over the CTAs in a fixed order.
+__global__ void bias_grad_reduce_kernel(const float* __restrict__ part, int nparts, int cout_pad, int cout,
+                                        float* __restrict__ db) {
     const int co = threadIdx.x;
     if (co >= cout) return;
     float s = 0.0f;
-    for (int p = 0; p < nparts; ++p) s += part[p * cout + co];
+    for (int p = 0; p < nparts; ++p) s += part[p * cout_pad + co];
     db[co] = s;
 }
 
@@ -630,6 +623,7 @@ int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int
     a.X = static_cast<const uint4*>(X);
     a.dZ = static_cast<const uint4*>(dZ);
     a.partial = partial;
+    a.db_part = db_part;
     a.B = B; a.H = H; a.W = W;
     a.rows_per_cta = (B * H + nparts - 1) / nparts;
     a.err = err;
@@ -642,9 +636,7 @@ int fvnet_conv3x3_wgrad(int cin_pad, int cout_pad, int cin, int cout, int B, int
     // parts actually used: CTAs whose row range is not empty
     const int used = (B * H + a.rows_per_cta - 1) / a.rows_per_cta;
     wgrad_reduce_kernel<<<(cout * cin * 9 + 255) / 256, 256, 0, st>>>(partial, used, cin_pad, cout_pad, cin, cout, dW);
-    bias_grad_partial_kernel<<<64, NT, 0, st>>>(static_cast<const uint4*>(dZ), (long long)B * H * W, cout_pad / 8,
-                                                cout, db_part);
-    bias_grad_reduce_kernel<<<1, 64, 0, st>>>(db_part, 64, cout, db);
+    bias_grad_reduce_kernel<<<1, 64, 0, st>>>(db_part, used, cout_pad, cout, db);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fv_internal_set_error(FVNET_ERR_CUDA, cudaGetErrorString(e));
     return FVNET_OK;

@@ -126,7 +126,7 @@ def test_conv_weight_gradient(B, H, W, ci, co, cip, cop):
     partial = torch.empty(parts * 9 * cip * cop, dtype=torch.float32, device="cuda")
     dW = torch.empty(co * ci * 9, dtype=torch.float32, device="cuda")
     db = torch.empty(co, dtype=torch.float32, device="cuda")
-    dbp = torch.empty(64 * co, dtype=torch.float32, device="cuda")
+    dbp = torch.empty(parts * cop, dtype=torch.float32, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     rc = L.fvnet_conv3x3_wgrad(cip, cop, ci, co, B, H, W, P(Xb), P(dZb), P(partial), P(dW), P(db), P(dbp), P(err), None)
     assert rc == 0, L.fv_last_error()
