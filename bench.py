@@ -433,7 +433,7 @@ def hybrid_leg(n_riemann=6, n_blast=6, n_kh=4, batch=128, frames=100, truth_n=10
     compared on the 64^2 grid (pareto.py).  Every method advances and is timed on a batch of `batch`
     held-out trajectories: the evaluated ones and more Riemann/blast initial conditions (indices
     300000+, first frames block-averaged from their initial states); errors are those of the
-    evaluated ones.  The equal-error verdict at each horizon: the coarsest plain resolution at least as
+    evaluated ones.  The equal-error comparison at each horizon: the coarsest plain resolution at least as
     accurate as the hybrid, and their GPU times per trajectory."""
     import torch
     pareto = importlib.import_module(f"{PKG}.pareto")
