@@ -331,14 +331,16 @@ struct WgradArgs {
 // contiguous bytes per pixel and consecutive pixels are 16 bytes apart, which is the canonical
 // no-swizzle MN-major layout (instruction descriptor major bits set; LBO = 128 bytes between groups
 // of 8 pixels, SBO = the chunk stride).  There are no operand transposes.
-// Input rows live in a 4-slot ring, each row stored twice (planes s and s + 4, s = (u + 1) mod 4 for
+// Input rows live in an 8-slot ring, each row stored twice (planes s and s + 8, s = (u + 1) mod 8 for
 // image row u), so that the rows y - 1, y, y + 1 and one more are always 4 consecutive planes of CC
 // chunks: the M rows (ky, ci) then have one chunk stride.  The fourth plane only feeds M rows past
-// 3 CIN, whose results are not used; it is the slot the next row's input is prefetched into while the
-// current row's MMAs run.  The output-gradient rows alternate between two buffers.
+// 3 CIN, whose results are not used.  An iteration takes two output rows of one image (one at an
+// image's or range's end) with one MMA commit and one CTA barrier; while its MMAs run, the next
+// iteration's new input rows are copied into slots that the MMAs read at most as an unused fourth
+// plane, and its output-gradient rows into the other of two buffers.
 __host__ __device__ constexpr size_t wgrad_mn_smem_bytes(int cin, int cout, int W) {
     // at least 46 KB: at most 4 CTAs per SM, so that their TMEM (up to 128 columns each) always fits
-    const size_t b = size_t(8) * (cin / 8) * (W + 2) * 16 + size_t(2) * (cout / 8) * W * 16 + 64;
+    const size_t b = size_t(16) * (cin / 8) * (W + 2) * 16 + size_t(4) * (cout / 8) * W * 16 + 64;
     return b < 46 * 1024 ? 46 * 1024 : b;
 }
 
@@ -350,9 +352,9 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
     constexpr uint32_t kCols = (3 * COUT) <= 32 ? 32 : ((3 * COUT) <= 64 ? 64 : 128);
     extern __shared__ __align__(1024) unsigned char smem[];
     const int W = a.W, H = a.H, W2 = W + 2;
-    uint4* Xs = reinterpret_cast<uint4*>(smem);    // [8 planes][CC][W + 2]: pixels x = -1 .. W
-    uint4* Ds = Xs + size_t(8) * CC * W2;          // [2][OC][W]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + size_t(2) * OC * W);
+    uint4* Xs = reinterpret_cast<uint4*>(smem);    // [16 planes][CC][W + 2]: pixels x = -1 .. W
+    uint4* Ds = Xs + size_t(16) * CC * W2;         // [2 buffers][2 rows][OC][W]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Ds + size_t(4) * OC * W);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int total = a.B * H;
@@ -365,11 +367,11 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
     }
     // input row u (image n, u in [-1, H], periodic) into its two planes, with the periodic x-neighbours
     auto stage_x = [&](int n, int u) {
-        const int yr = (u + H) % H, s = (u + 1) & 3;
+        const int yr = (u + H) % H, s = (u + 1) & 7;
         const uint4* src = a.X + size_t(n * H + yr) * W * CC;
         for (int e = tid; e < W * CC; e += NT) {
             const int x = e / CC, cc = e - x * CC;
-            for (int p = s; p < 8; p += 4) {
+            for (int p = s; p < 16; p += 8) {
                 uint4* row = Xs + (size_t(p) * CC + cc) * W2;
                 tc::cp_async16(row + x + 1, src + e);
                 if (x == W - 1) tc::cp_async16(row, src + e);
@@ -377,18 +379,20 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
             }
         }
     };
-    auto stage_dz = [&](int n, int y, int buf) {  // output-gradient row y into buffer buf: [oc][x]
+    auto stage_dz = [&](int n, int y, int buf, int j) {  // output-gradient row y into buffer buf, row j: [oc][x]
         const uint4* src = a.dZ + size_t(n * H + y) * W * OC;
         for (int e = tid; e < W * OC; e += NT) {
             const int x = e / OC, oc = e - x * OC;
-            tc::cp_async16(Ds + (size_t(buf) * OC + oc) * W + x, src + e);
+            tc::cp_async16(Ds + ((size_t(buf) * 2 + j) * OC + oc) * W + x, src + e);
         }
     };
+    // output rows an iteration starting at `row` takes: two of one image, one at an image's or range's end
+    auto rows_in = [&](int row) { return (row + 1 < r1 && (row + 1) % H != 0) ? 2 : 1; };
     int cur = 0;
     if (r0 < r1) {
-        const int n = r0 / H, y = r0 % H;
-        stage_x(n, y - 1); stage_x(n, y); stage_x(n, y + 1);
-        stage_dz(n, y, 0);
+        const int n = r0 / H, y = r0 % H, k = rows_in(r0);
+        for (int u = y - 1; u <= y + k; ++u) stage_x(n, u);
+        for (int j = 0; j < k; ++j) stage_dz(n, y + j, 0, j);
     }
     tc::cp_async_wait_all();
     tc::fence_proxy_async_smem();
@@ -402,44 +406,52 @@ __global__ void __launch_bounds__(NT) conv3x3_wgrad_mn_kernel(WgradArgs a) {
     uint32_t phase = 0;
     bool ok = true;
     float bacc = 0.0f;
-    for (int row = r0; row < r1 && ok; ++row) {
-        const int n = row / H, y = row % H;
+    for (int row = r0; row < r1;) {
+        const int n = row / H, y = row % H, k = rows_in(row);
         if (tid == 0) {
-            const int p0 = y & 3;  // planes p0 .. p0 + 2 hold rows y - 1, y, y + 1
-            for (int kx = 0; kx < 3; ++kx)
-                for (int ks = 0; ks < W / 16; ++ks) {
-                    const uint32_t aa = xb + (uint32_t(p0 * CC) * W2 + 16 * ks + kx) * 16;
-                    const uint32_t ba = db + (uint32_t(cur * OC) * W + 16 * ks) * 16;
-                    tc::mma_bf16(tmem + kx * COUT, tc::smem_desc(aa, 128, sbo_a), tc::smem_desc(ba, 128, sbo_b), idesc,
-                                 (row > r0 || ks > 0) ? 1u : 0u);
-                }
+            for (int j = 0; j < k; ++j) {
+                const int p0 = (y + j) & 7;  // planes p0 .. p0 + 2 hold rows y + j - 1 .. y + j + 1
+                for (int kx = 0; kx < 3; ++kx)
+                    for (int ks = 0; ks < W / 16; ++ks) {
+                        const uint32_t aa = xb + (uint32_t(p0 * CC) * W2 + 16 * ks + kx) * 16;
+                        const uint32_t ba = db + (uint32_t((cur * 2 + j) * OC) * W + 16 * ks) * 16;
+                        tc::mma_bf16(tmem + kx * COUT, tc::smem_desc(aa, 128, sbo_a), tc::smem_desc(ba, 128, sbo_b),
+                                     idesc, (row > r0 || j > 0 || ks > 0) ? 1u : 0u);
+                    }
+            }
             tc::mma_commit(bar);
         }
-        const int nrow = row + 1;
+        const int nrow = row + k;
         const bool has_next = nrow < r1, next_cont = has_next && (nrow % H) != 0;
-        if (next_cont) {  // during the MMAs: input row y + 2 (the slot of the unused fourth plane), dZ row y + 1
-            stage_x(n, y + 2);
-            stage_dz(n, y + 1, cur ^ 1);
+        const int k2 = has_next ? rows_in(nrow) : 0;
+        if (next_cont) {  // during the MMAs: the next iteration's new input rows and its dZ rows
+            for (int u = y + k + 1; u <= y + k + k2; ++u) stage_x(n, u);
+            for (int j = 0; j < k2; ++j) stage_dz(n, y + k + j, cur ^ 1, j);
         }
-        {  // the bias gradient: thread t sums channel t % COUT over pixels t / COUT, + NT / COUT, .. of the row
-            const __nv_bfloat16* dz = reinterpret_cast<const __nv_bfloat16*>(Ds + size_t(cur) * OC * W);
+        {  // the bias gradient: thread t sums channel t % COUT over pixels t / COUT, + NT / COUT, .. of the rows
             const int co = tid % COUT;
-            for (int x = tid / COUT; x < W; x += NT / COUT) bacc += __bfloat162float(dz[(size_t(co / 8) * W + x) * 8 + co % 8]);
+            for (int j = 0; j < k; ++j) {
+                const __nv_bfloat16* dz = reinterpret_cast<const __nv_bfloat16*>(Ds + size_t(cur * 2 + j) * OC * W);
+                for (int x = tid / COUT; x < W; x += NT / COUT) bacc += __bfloat162float(dz[(size_t(co / 8) * W + x) * 8 + co % 8]);
+            }
         }
         ok = tc::mbar_wait_bounded(bar, phase, a.err);
         phase ^= 1;
         tc::fence_after_sync();
-        if (has_next && !next_cont) {  // a new image: its three rows, now that the MMAs are done
+        if (has_next && !next_cont) {  // a new image: its rows, now that the MMAs are done
             const int n2 = nrow / H;
-            stage_x(n2, -1); stage_x(n2, 0); stage_x(n2, 1);
-            stage_dz(n2, 0, cur ^ 1);
+            for (int u = -1; u <= k2; ++u) stage_x(n2, u);
+            for (int j = 0; j < k2; ++j) stage_dz(n2, j, cur ^ 1, j);
         }
         tc::cp_async_wait_all();
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
-        __syncthreads();  // the next row's data is visible
+        const int all_ok = __syncthreads_and(ok ? 1 : 0);  // the next iteration's data is visible
         tc::fence_after_sync();
+        ok = all_ok != 0;
+        if (!ok) break;  // a wait ran out (the error flag is set): the whole CTA leaves
         cur ^= 1;
+        row = nrow;
     }
     if (ok && r0 < r1) {
         for (int kx = 0; kx < 3; ++kx) {
